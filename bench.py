@@ -1,0 +1,333 @@
+#!/usr/bin/env python
+"""Benchmark: full N-Queens count N=21 (pregen depth 7) on one B200.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl nqb|reference]
+
+One step = one full count: every state of the depth-7 pool searched to the last row.
+`value` is search nodes/s with the pool already resident in HBM (kernel time by CUDA
+events on the launching stream); `e2e` is the same metric through the public C ABI
+call nqb_count_ex(21, 7) with host buffers: pool generation, host->device copy, kernel
+and result read-back inside the timed region.  Prints one JSON line on rank 0.
+
+`--impl reference` times the reference's own CPU path (oracle/_ref, built from the
+reference's sources) on bounded stride samples of the same pool with every host core,
+and, for comparison, the reference CUDA build on the same GPU.
+
+Multi-GPU: the north star is one GPU, so N > 1 runs N independent replicas (weak
+scaling, no collective on the data path); the step time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+KAT = {13: 73712, 17: 95815104, 18: 666090624, 19: 4968057848, 20: 39029188884, 21: 314666222712,
+       22: 2691008701644}
+INT_OPS_PER_NODE = 15  # algorithmic INT32 lane-ops per node (fixed convention)
+METRIC = "N=21 count wall-time & nodes/s on 1 GPU: batched+learned vs plain, bit-exact"
+
+
+def load_pkg():
+    from __graft_entry__ import _import_pkg
+    return _import_pkg()
+
+
+def rank_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device, self.rows, self._stop = device, [], threading.Event()
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def sm_count(torch, dev):
+    return torch.cuda.get_device_properties(dev).multi_processor_count
+
+
+def roofline(nodes, seconds, sms, max_mhz, traffic):
+    achieved = nodes / seconds * INT_OPS_PER_NODE / 1e12
+    peak = sms * 4 * 32 * max_mhz * 1e6 / 1e12
+    return {"bound": "int32-issue", "achieved": round(achieved, 3), "peak": round(peak, 3),
+            "unit": "Tlane-op/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+            "peak_source": f"nominal issue peak: {sms} SMs x 4 SMSP x 32 lanes x {max_mhz:.0f} MHz",
+            "ops_per_node": INT_OPS_PER_NODE}
+
+
+def profile_traffic(kernel, n, d):
+    """DRAM bytes per launch recorded from an ncu capture in profiles/ (or None)."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith(f"n{n}d{d} "):
+            return int(line.split()[1])
+    return None
+
+
+def cpu_baseline_sample(n, d, target_s, steps=1, offset0=0):
+    """Times the reference's host DFS (oracle/_ref) on stride samples of the pool with every
+    host core; falls back to the oracle port (single core) when the harness is absent."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import nqo
+    cores = os.cpu_count() or 1
+    results = []
+    if nqo.ref_available(n):
+        probe = nqo.run_ref(n, "cpu", d, cores, 1 << 18, 0)[0]
+        rate = probe["nodes"] / max(probe["seconds"], 1e-3)
+        total_est = rate * 0 + probe["nodes"] * probe["states"] / max(probe["sampled"], 1)
+        stride = max(1, int(total_est / max(rate * target_s, 1.0)))
+        for s in range(steps):
+            r = nqo.run_ref(n, "cpu", d, cores, stride, (offset0 + s) % stride)[0]
+            results.append(dict(r, stride=stride, offset=(offset0 + s) % stride))
+        kind, used = "reference", cores
+    else:
+        probe = nqo.replay_pool(n, d, 1 << 18, 0)
+        t0 = time.perf_counter()
+        nqo.replay_pool(n, d, 1 << 18, 1)
+        rate = probe["nodes"] / max(time.perf_counter() - t0, 1e-3)
+        states = nqo.pool_size(n, d)[0]
+        stride = max(1, int(probe["nodes"] * (states / max(probe["sampled"], 1)) / max(rate * target_s, 1.0)))
+        for s in range(steps):
+            t0 = time.perf_counter()
+            r = nqo.replay_pool(n, d, stride, (offset0 + s) % stride)
+            results.append(dict(r, seconds=time.perf_counter() - t0, stride=stride, offset=(offset0 + s) % stride,
+                                states=states))
+        kind, used = "port", 1
+    return results, kind, used
+
+
+def run_nqb(args):
+    import torch
+    import torch.distributed as dist
+    rank, world, local = rank_env()
+    dev = local
+    torch.cuda.set_device(dev)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", dev))
+    nqb = load_pkg()
+    n, d = args.n, args.depth
+    pool = nqb.generate_pool(n, d)
+    states = len(pool)
+    stack_depth = n - d - 1
+    d_pool = torch.from_numpy(pool.view(np.uint8)).to(f"cuda:{dev}")
+    d_out = torch.zeros((max(args.steps, args.warmup), 4), dtype=torch.int64, device=f"cuda:{dev}")
+    stream = torch.cuda.current_stream(dev)
+    sptr = stream.cuda_stream
+
+    def step(i):
+        nqb.plain_launch(d_pool.data_ptr(), states, d_out[i].data_ptr(), block_size=args.block,
+                         stack_depth=stack_depth, stream=sptr)
+
+    # warm-up (untimed), also the correctness check
+    d_out.zero_()
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize(dev)
+    w = d_out.cpu().numpy().astype(np.uint64)
+    count, nodes = int(w[0, 0]), int(w[0, 1])
+    assert all(int(w[i, 3]) == 0 for i in range(args.warmup)), "device error flag set"
+    assert all(int(w[i, 0]) == count and int(w[i, 1]) == nodes for i in range(args.warmup))
+    if n in KAT:
+        assert count == KAT[n], (count, KAT[n])
+
+    # timed region: K full counts, pool resident in HBM (630 MB > L2 at n=21 d=7)
+    d_out.zero_()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(dev) as clk:
+        ev0.record(stream)
+        for i in range(args.steps):
+            step(i)
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+    ms = ev0.elapsed_time(ev1)
+    res = d_out.cpu().numpy().astype(np.uint64)
+    assert all(int(res[i, 0]) == count and int(res[i, 1]) == nodes for i in range(args.steps))
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = nodes * world / (ms_step / 1e3)
+
+    # e2e: the public C ABI call with host buffers, every step
+    e2e = None
+    if not args.skip_e2e:
+        nqb.count_ex(n, d, device=dev)  # warm-up of the call path
+        if world > 1:
+            dist.barrier()
+        walls, gen, h2d, ker = [], [], [], []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            c, st = nqb.count_ex(n, d, device=dev)
+            walls.append(time.perf_counter() - t0)
+            assert c == count
+            gen.append(st["gen_ms"]), h2d.append(st["h2d_ms"]), ker.append(st["kernel_ms"])
+        wall = max(walls) if world == 1 else None
+        if world > 1:
+            t = torch.tensor([max(walls)], device=f"cuda:{dev}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            wall = float(t.item())
+        e2e = {"value": nodes * world / (sum(walls) / len(walls)), "unit": "nodes/s",
+               "h2d_bytes_per_step": states * 16, "d2h_bytes_per_step": 32,
+               "wall_ms_per_step": round(1e3 * sum(walls) / len(walls), 3), "max_wall_ms": round(1e3 * wall, 3),
+               "gen_ms": round(float(np.mean(gen)), 3), "h2d_ms": round(float(np.mean(h2d)), 3),
+               "kernel_ms": round(float(np.mean(ker)), 3), "api": "nqb_count_ex"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        rs, kind, cores = cpu_baseline_sample(n, d, args.cpu_seconds)
+        r = rs[0]
+        cpu = {"value": r["nodes"] / r["seconds"], "unit": "nodes/s", "cores": cores, "kind": kind,
+               "sample": f"every {r['stride']}th state of the n={n} d={d} pool ({r['sampled']} of {r['states']} "
+                         f"states, {r['nodes']} nodes, {r['seconds']:.2f} s)"}
+        # the same sample through the library: bit-exact check of the baseline's count
+        samp = pool[r["offset"]::r["stride"]]
+        got, stc = nqb.solve_states(samp, device=dev)
+        cpu["sample_count_match"] = bool(got == r["count"] and stc["nodes"] == r["nodes"])
+
+    if rank == 0:
+        sms = sm_count(torch, dev)
+        ck = clk.summary()
+        max_mhz = ck["sm_max_mhz"] or 1965.0
+        line = {
+            "metric": METRIC, "value": round(value, 1), "unit": "nodes/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic (the full depth-7 pool of the N=21 board)",
+            "config": {"workload": f"full count N={n}, pregen depth {d}", "n": n, "depth": d, "form": "plain",
+                       "states": states, "nodes": nodes, "count": count, "block": args.block or 128,
+                       "parallelism": f"replicas{world}" if world > 1 else "single",
+                       "l2": f"inputs larger than L2 (pool {states * 16 / 1e6:.0f} MB)"},
+            "e2e": e2e,
+            "roofline": roofline(nodes, ms_step / 1e3, sms, max_mhz,
+                                 profile_traffic("plain_search_kernel", n, d)),
+            "cpu_baseline": cpu,
+            "clocks": ck,
+            "gpu_launches": args.steps * (1 + (states - 1) // (1 << 30)),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    rank, world, local = rank_env()
+    if rank != 0:
+        return
+    n, d = args.n, args.depth
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import nqo
+    step_s = args.ref_step_seconds
+    rs, kind, cores = cpu_baseline_sample(n, d, step_s, steps=args.warmup + args.steps)
+    timed = rs[args.warmup:]
+    nodes = sum(r["nodes"] for r in timed)
+    secs = sum(r["seconds"] for r in timed)
+    value = nodes / secs
+    sample = (f"per step every {timed[0]['stride']}th state of the n={n} d={d} pool (offsets "
+              f"{[r['offset'] for r in timed]}), {nodes} nodes in {secs:.2f} s")
+    line = {"metric": METRIC, "impl": "reference", "value": round(value, 1), "unit": "nodes/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * secs / len(timed), 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (stride samples of the depth-7 pool of the N=21 board)",
+            "config": {"workload": f"full count N={n}, pregen depth {d}", "n": n, "depth": d,
+                       "form": "reference host DFS (locked_advance_nq_state)"},
+            "cpu_baseline": {"value": round(value, 1), "unit": "nodes/s", "cores": cores, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": round(value, 1), "unit": "nodes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if args.ref_cuda and nqo.ref_available(n):
+        line["reference_cuda"] = reference_cuda(nqo, n, d)
+    print(json.dumps(line), flush=True)
+
+
+def reference_cuda(nqo, n, d):
+    """The reference CUDA build (kern_doitall_v2_regld via gpu_solver_driver) on this GPU."""
+    import re
+    t0 = time.perf_counter()
+    p = subprocess.run([nqo.ref_harness_path(n), "gpu", str(d), "1"], capture_output=True, text=True, timeout=3600)
+    wall = time.perf_counter() - t0
+    if p.returncode != 0:
+        return {"unavailable": f"reference CUDA run exited {p.returncode}"}
+    js = [json.loads(l[9:]) for l in p.stdout.splitlines() if l.startswith("NQO_JSON ")]
+    km = [float(x) for x in re.findall(r"Time taken: ([0-9.]+)ms", p.stdout)]
+    r = js[-1] if js else {}
+    out = {"count": r.get("count"), "count_ok": r.get("count") == KAT.get(n), "kernel_ms": km[-1] if km else None,
+           "driver_ms": round(1e3 * r.get("driver_seconds", 0), 3), "gen_ms": round(1e3 * r.get("gen_seconds", 0), 3),
+           "process_wall_s": round(wall, 3)}
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="nqb", choices=["nqb", "reference"])
+    ap.add_argument("--n", type=int, default=21)
+    ap.add_argument("--depth", type=int, default=7)
+    ap.add_argument("--block", type=int, default=0)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ref-step-seconds", type=float, default=8.0)
+    ap.add_argument("--ref-cuda", type=int, default=1)
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 1:
+        args.warmup = 1
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_nqb(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,249 @@
+"""Python binding of libnqb.so, the B200 N-Queens counter (C ABI in include/nqb.h).
+
+Mirrors the reference's host calls (fillpant/GPU-N-Queens):
+  count(n, depth)            nq_generate_states_rowlock + solve()/gpu_solver_driver
+                             (n_queens.cuh:119, NQ_solver.cu:192-209, GPU_NQueens.cuh:13)
+  generate_pool(n, depth)    nq_generate_states_rowlock (n_queens.cuh:119)
+  solve_ref_states(...)      gpu_solver_driver on reference nq_state_t records
+The reference aborts on errors (FAIL_IF / CHECK_CUDA_ERROR, deffinitions.cuh:148-156);
+here every failure raises NQBError carrying the library's status code.  There is no
+CPU fallback: if libnqb.so is missing, loading raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libnqb.so")
+INCLUDE_DIR = os.path.join(os.path.dirname(HERE), "include")
+
+STATE_DTYPE = np.dtype([("cols", "<u4"), ("ldiag", "<u4"), ("rdiag", "<u4"),
+                        ("row", "u1"), ("n", "u1"), ("weight", "u1"), ("flags", "u1")])
+assert STATE_DTYPE.itemsize == 16
+
+OK, E_INVALID, E_NOMEM, E_CUDA, E_NODEVICE, E_RANGE, E_STALL, E_DEVICE, E_MODEL = range(9)
+FORM_PLAIN, FORM_BATCHED = 0, 1
+MIN_N, MAX_N = 4, 31
+
+
+class NQBError(RuntimeError):
+    def __init__(self, status, what=""):
+        self.status = status
+        super().__init__(f"{what}: {strerror(status)} (status {status})" if what else strerror(status))
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("form", ctypes.c_int), ("block_size", ctypes.c_int),
+                ("count_unit_nodes", ctypes.c_int), ("use_model", ctypes.c_int),
+                ("split_depth", ctypes.c_int), ("reserved", ctypes.c_int * 10)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("states", ctypes.c_uint64), ("nodes", ctypes.c_uint64), ("unit_nodes", ctypes.c_uint64),
+                ("gen_ms", ctypes.c_double), ("h2d_ms", ctypes.c_double), ("kernel_ms", ctypes.c_double),
+                ("wall_ms", ctypes.c_double), ("pregen_depth", ctypes.c_uint32),
+                ("kernel_launches", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 6)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        if d["unit_nodes"] == 2 ** 64 - 1:
+            d["unit_nodes"] = None
+        return d
+
+
+_lib = None
+
+
+def build():
+    import subprocess
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    """Loads libnqb.so (raises OSError when it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"{LIB_PATH} is missing: run `make -C {HERE}` (there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        u64p = ctypes.POINTER(ctypes.c_uint64)
+        vp = ctypes.c_void_p
+        sig = {
+            "nqb_default_opts": (None, [ctypes.POINTER(Opts)]),
+            "nqb_strerror": (ctypes.c_char_p, [ctypes.c_int]),
+            "nqb_version": (ctypes.c_int, []),
+            "nqb_device_check": (ctypes.c_int, [ctypes.c_int]),
+            "nqb_count": (ctypes.c_int, [ctypes.c_uint, ctypes.c_uint, u64p]),
+            "nqb_count_ex": (ctypes.c_int, [ctypes.c_uint, ctypes.c_uint, ctypes.POINTER(Opts), u64p,
+                                            ctypes.POINTER(Stats)]),
+            "nqb_generate_pool": (ctypes.c_int, [ctypes.c_uint, ctypes.c_uint, ctypes.POINTER(vp), u64p]),
+            "nqb_generate_pool_into": (ctypes.c_int, [ctypes.c_uint, ctypes.c_uint, vp, ctypes.c_uint64, u64p]),
+            "nqb_pool_weighted_size": (ctypes.c_int, [ctypes.c_uint, ctypes.c_uint, u64p]),
+            "nqb_free": (None, [vp]),
+            "nqb_solve_states": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.POINTER(Opts), u64p,
+                                                ctypes.POINTER(Stats)]),
+            "nqb_solve_batch": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.POINTER(Opts), vp,
+                                               ctypes.POINTER(Stats)]),
+            "nqb_ref_state_size": (ctypes.c_size_t, [ctypes.c_uint]),
+            "nqb_states_from_ref": (ctypes.c_int, [ctypes.c_uint, vp, ctypes.c_uint64, ctypes.c_int, vp]),
+            "nqb_solve_ref_states": (ctypes.c_int, [ctypes.c_uint, vp, ctypes.c_uint64, ctypes.c_uint,
+                                                    ctypes.POINTER(Opts), u64p]),
+            "nqb_sample_boards": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint, ctypes.c_uint,
+                                                 ctypes.c_uint, ctypes.c_uint, vp]),
+            "nqb_plain_launch": (ctypes.c_int, [vp, ctypes.c_uint64, vp, ctypes.c_int, ctypes.c_int,
+                                                ctypes.c_uint, vp]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def strerror(status):
+    try:
+        return lib().nqb_strerror(status).decode()
+    except OSError:
+        return f"status {status}"
+
+
+def _check(status, what):
+    if status != OK:
+        raise NQBError(status, what)
+
+
+def make_opts(device=0, form=FORM_PLAIN, block_size=0, count_unit_nodes=False, use_model=False,
+              split_depth=-1):
+    o = Opts()
+    lib().nqb_default_opts(ctypes.byref(o))
+    o.device, o.form, o.block_size = device, form, block_size
+    o.count_unit_nodes, o.use_model, o.split_depth = int(count_unit_nodes), int(use_model), split_depth
+    return o
+
+
+def device_check(device=0):
+    return lib().nqb_device_check(device)
+
+
+def count(n, depth, **opts):
+    """Mirror-weighted number of n-queens solutions via a depth-row pool (the drop-in)."""
+    c = ctypes.c_uint64(0)
+    _check(lib().nqb_count_ex(n, depth, ctypes.byref(make_opts(**opts)), ctypes.byref(c), None),
+           f"nqb_count({n}, {depth})")
+    return c.value
+
+
+def count_ex(n, depth, **opts):
+    """(count, stats dict) for the (n, depth) pool."""
+    c = ctypes.c_uint64(0)
+    st = Stats()
+    _check(lib().nqb_count_ex(n, depth, ctypes.byref(make_opts(**opts)), ctypes.byref(c), ctypes.byref(st)),
+           f"nqb_count_ex({n}, {depth})")
+    return c.value, st.as_dict()
+
+
+def pool_size(n, depth):
+    c = ctypes.c_uint64(0)
+    _check(lib().nqb_generate_pool_into(n, depth, None, 0, ctypes.byref(c)), "nqb_generate_pool_into")
+    return c.value
+
+
+def pool_weighted_size(n, depth):
+    w = ctypes.c_uint64(0)
+    _check(lib().nqb_pool_weighted_size(n, depth, ctypes.byref(w)), "nqb_pool_weighted_size")
+    return w.value
+
+
+def generate_pool(n, depth):
+    """The (n, depth) pool as a numpy array of STATE_DTYPE, in the reference's order."""
+    cnt = pool_size(n, depth)
+    out = np.zeros(max(cnt, 1), dtype=STATE_DTYPE)
+    got = ctypes.c_uint64(0)
+    _check(lib().nqb_generate_pool_into(n, depth, out.ctypes.data, cnt, ctypes.byref(got)), "nqb_generate_pool_into")
+    return out[:got.value]
+
+
+def generate_pool_alloc(n, depth):
+    """Same pool through nqb_generate_pool (library-allocated, released with nqb_free)."""
+    p = ctypes.c_void_p()
+    c = ctypes.c_uint64(0)
+    _check(lib().nqb_generate_pool(n, depth, ctypes.byref(p), ctypes.byref(c)), "nqb_generate_pool")
+    try:
+        buf = (ctypes.c_uint8 * (16 * c.value)).from_address(p.value) if c.value else b""
+        return np.frombuffer(bytes(buf), dtype=STATE_DTYPE).copy()
+    finally:
+        lib().nqb_free(p)
+
+
+def solve_states(states, **opts):
+    """(total, stats) for library states in host memory."""
+    states = np.ascontiguousarray(states, dtype=STATE_DTYPE)
+    t = ctypes.c_uint64(0)
+    st = Stats()
+    _check(lib().nqb_solve_states(states.ctypes.data if len(states) else None, len(states),
+                                  ctypes.byref(make_opts(**opts)), ctypes.byref(t), ctypes.byref(st)),
+           "nqb_solve_states")
+    return t.value, st.as_dict()
+
+
+def solve_batch(boards, **opts):
+    """(per-board weighted counts as uint64 array, stats)."""
+    boards = np.ascontiguousarray(boards, dtype=STATE_DTYPE)
+    out = np.zeros(max(len(boards), 1), dtype=np.uint64)
+    st = Stats()
+    _check(lib().nqb_solve_batch(boards.ctypes.data if len(boards) else None, len(boards),
+                                 ctypes.byref(make_opts(**opts)), out.ctypes.data, ctypes.byref(st)),
+           "nqb_solve_batch")
+    return out[:len(boards)], st.as_dict()
+
+
+BATCH_SEED = 0x4E51554545534231  # uneven partial boards: 65,536 boards, n 16..20, depth 3..7
+MODEL_SEED = 0x4E5131384C524E31  # cost-model training set: n = 18, depth 4..8
+
+
+def sample_boards(seed, count, n_min, n_max, d_min, d_max):
+    """Seeded random valid partial boards (see nqb_sample_boards)."""
+    out = np.zeros(max(count, 1), dtype=STATE_DTYPE)
+    _check(lib().nqb_sample_boards(seed, count, n_min, n_max, d_min, d_max, out.ctypes.data), "nqb_sample_boards")
+    return out[:count]
+
+
+def ref_state_size(n):
+    return int(lib().nqb_ref_state_size(n))
+
+
+def states_from_ref(n, ref_bytes, mirror_weight=True):
+    sz = ref_state_size(n)
+    ref_bytes = np.ascontiguousarray(np.frombuffer(ref_bytes, dtype=np.uint8))
+    cnt = len(ref_bytes) // sz
+    out = np.zeros(max(cnt, 1), dtype=STATE_DTYPE)
+    _check(lib().nqb_states_from_ref(n, ref_bytes.ctypes.data, cnt, int(mirror_weight), out.ctypes.data),
+           "nqb_states_from_ref")
+    return out[:cnt]
+
+
+def solve_ref_states(n, ref_bytes, locked_row, **opts):
+    """gpu_solver_driver replacement on reference nq_state_t records."""
+    sz = ref_state_size(n)
+    ref_bytes = np.ascontiguousarray(np.frombuffer(ref_bytes, dtype=np.uint8))
+    t = ctypes.c_uint64(0)
+    _check(lib().nqb_solve_ref_states(n, ref_bytes.ctypes.data, len(ref_bytes) // sz, locked_row,
+                                      ctypes.byref(make_opts(**opts)), ctypes.byref(t)), "nqb_solve_ref_states")
+    return t.value
+
+
+def plain_launch(d_states_ptr, count, d_out_ptr, block_size=0, count_unit_nodes=False, stack_depth=0,
+                 stream=0):
+    """Launches the plain kernel on device pointers (see nqb_plain_launch)."""
+    _check(lib().nqb_plain_launch(d_states_ptr, count, d_out_ptr, block_size, int(count_unit_nodes),
+                                  stack_depth, stream or None), "nqb_plain_launch")
+
+
+def header_symbols():
+    """Names of the functions include/nqb.h declares."""
+    import re
+    src = open(os.path.join(INCLUDE_DIR, "nqb.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(nqb_[a-z0-9_]+)\s*\(", src)))

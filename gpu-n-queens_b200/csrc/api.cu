@@ -1,0 +1,329 @@
+// C ABI of libnqb.so (include/nqb.h): argument checks, device buffers, streams and timing
+// around the pool generator and the search kernels.  Replaces the reference's solve()
+// (NQ_solver.cu:192-209) and gpu_solver_driver (GPU_NQueens.cu:56-175); unlike those it
+// never exits the process and frees everything it allocated on every path.
+#include <chrono>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "nqb_internal.h"
+
+namespace nqb {
+
+int cuda_status(cudaError_t e) {
+    if (e == cudaSuccess) return NQB_OK;
+    if (e == cudaErrorMemoryAllocation) return NQB_E_NOMEM;
+    if (e == cudaErrorNoDevice || e == cudaErrorInvalidDevice || e == cudaErrorInsufficientDriver)
+        return NQB_E_NODEVICE;
+    return NQB_E_CUDA;
+}
+
+namespace {
+
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// Device-call scope: selects the device, owns a stream, timing events and buffers,
+// and restores the caller's device on exit.
+class Scope {
+   public:
+    int status = NQB_OK;
+    cudaStream_t stream = nullptr;
+
+    explicit Scope(int device) {
+        cudaGetDevice(&prev_);
+        status = nqb_device_check(device);
+        if (status != NQB_OK) return;
+        if ((status = cuda_status(cudaSetDevice(device))) != NQB_OK) return;
+        status = cuda_status(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    }
+    ~Scope() {
+        if (stream) cudaStreamSynchronize(stream);
+        for (void* p : bufs_) cudaFree(p);
+        for (cudaEvent_t e : events_) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+        cudaSetDevice(prev_);
+    }
+    template <class T>
+    int alloc(T** p, size_t bytes) {
+        void* v = nullptr;
+        const int s = cuda_status(cudaMalloc(&v, bytes ? bytes : 16));
+        if (s != NQB_OK) return s;
+        bufs_.push_back(v);
+        *p = static_cast<T*>(v);
+        return NQB_OK;
+    }
+    int event(cudaEvent_t* e) {
+        const int s = cuda_status(cudaEventCreate(e));
+        if (s == NQB_OK) events_.push_back(*e);
+        return s;
+    }
+    Scope(const Scope&) = delete;
+    Scope& operator=(const Scope&) = delete;
+
+   private:
+    int prev_ = 0;
+    std::vector<void*> bufs_;
+    std::vector<cudaEvent_t> events_;
+};
+
+#define NQB_TRY(expr)                   \
+    do {                                \
+        const int s_ = (expr);          \
+        if (s_ != NQB_OK) return s_;    \
+    } while (0)
+
+nqb_opts resolve(const nqb_opts* o) {
+    nqb_opts r;
+    nqb_default_opts(&r);
+    if (o) r = *o;
+    return r;
+}
+
+bool state_ok(const nqb_state& s) {
+    if (s.n < 1 || s.n > NQB_MAX_N || s.flags != 0) return false;
+    return (s.cols & ~board_mask(s.n)) == 0;
+}
+
+// Solves `count` host states on the device; fills totals {count, nodes, unit, err}
+// and, if per_state != nullptr, per-state weighted counts.
+int solve_host_states(Scope& sc, const nqb_state* states, uint64_t count, const nqb_opts& o,
+                      unsigned long long totals[4], uint64_t* per_state, nqb_stats* st) {
+    for (uint64_t i = 0; i < count; ++i)
+        if (!state_ok(states[i])) return NQB_E_INVALID;
+    const unsigned depth = max_stack_depth(states, count);
+    nqb_state* d_states = nullptr;
+    unsigned long long* d_out = nullptr;
+    unsigned long long* d_per = nullptr;
+    NQB_TRY(sc.alloc(&d_states, count * sizeof(nqb_state)));
+    NQB_TRY(sc.alloc(&d_out, 4 * sizeof(unsigned long long)));
+    if (per_state) NQB_TRY(sc.alloc(&d_per, count * sizeof(unsigned long long)));
+    cudaEvent_t e0, e1, e2;
+    NQB_TRY(sc.event(&e0));
+    NQB_TRY(sc.event(&e1));
+    NQB_TRY(sc.event(&e2));
+    NQB_TRY(cuda_status(cudaEventRecord(e0, sc.stream)));
+    NQB_TRY(cuda_status(
+        cudaMemcpyAsync(d_states, states, count * sizeof(nqb_state), cudaMemcpyHostToDevice, sc.stream)));
+    NQB_TRY(cuda_status(cudaMemsetAsync(d_out, 0, 4 * sizeof(unsigned long long), sc.stream)));
+    NQB_TRY(cuda_status(cudaEventRecord(e1, sc.stream)));
+    unsigned launches = 0;
+    NQB_TRY(launch_plain(d_states, count, d_out, d_per, o.block_size, o.count_unit_nodes != 0, depth, sc.stream,
+                         &launches));
+    NQB_TRY(cuda_status(cudaEventRecord(e2, sc.stream)));
+    NQB_TRY(cuda_status(cudaMemcpyAsync(totals, d_out, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                        sc.stream)));
+    if (per_state)
+        NQB_TRY(cuda_status(cudaMemcpyAsync(per_state, d_per, count * sizeof(unsigned long long),
+                                            cudaMemcpyDeviceToHost, sc.stream)));
+    NQB_TRY(cuda_status(cudaStreamSynchronize(sc.stream)));
+    if (totals[3]) return NQB_E_DEVICE;
+    if (st) {
+        float h2d = 0, ker = 0;
+        cudaEventElapsedTime(&h2d, e0, e1);
+        cudaEventElapsedTime(&ker, e1, e2);
+        st->states = count;
+        st->nodes = totals[1];
+        st->unit_nodes = o.count_unit_nodes ? totals[2] : UINT64_MAX;
+        st->h2d_ms = h2d;
+        st->kernel_ms = ker;
+        st->kernel_launches = launches;
+    }
+    return NQB_OK;
+}
+
+void* aligned_host_alloc(size_t bytes) {
+    void* p = nullptr;
+    if (posix_memalign(&p, 64, bytes ? bytes : 64)) return nullptr;
+    return p;
+}
+
+}  // namespace
+}  // namespace nqb
+
+using namespace nqb;
+
+extern "C" {
+
+void nqb_default_opts(nqb_opts* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->device = 0;
+    o->form = NQB_FORM_PLAIN;
+    o->block_size = 0;
+    o->split_depth = -1;
+}
+
+const char* nqb_strerror(int s) {
+    switch (s) {
+        case NQB_OK: return "ok";
+        case NQB_E_INVALID: return "invalid argument";
+        case NQB_E_NOMEM: return "out of memory";
+        case NQB_E_CUDA: return "CUDA runtime error";
+        case NQB_E_NODEVICE: return "no usable sm_100 CUDA device";
+        case NQB_E_RANGE: return "size beyond a supported limit";
+        case NQB_E_STALL: return "device-side bounded wait ran out";
+        case NQB_E_DEVICE: return "device-side check failed";
+        case NQB_E_MODEL: return "learned cost model missing or not trained";
+        default: return "unknown status";
+    }
+}
+
+int nqb_version(void) { return NQB_VERSION; }
+
+int nqb_device_check(int device) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return NQB_E_NODEVICE;
+    }
+    if (device < 0 || device >= n) return NQB_E_NODEVICE;
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, device) != cudaSuccess) return NQB_E_NODEVICE;
+    if (p.major != 10 || p.warpSize != 32 || p.computeMode == cudaComputeModeProhibited) return NQB_E_NODEVICE;
+    return NQB_OK;
+}
+
+void nqb_free(void* p) { std::free(p); }
+
+int nqb_generate_pool_into(unsigned n, unsigned depth, nqb_state* buf, uint64_t capacity, uint64_t* count) {
+    if (!count) return NQB_E_INVALID;
+    return generate_pool(n, depth, buf, buf ? capacity : 0, count, nullptr);
+}
+
+int nqb_pool_weighted_size(unsigned n, unsigned depth, uint64_t* weighted) {
+    if (!weighted) return NQB_E_INVALID;
+    uint64_t c = 0;
+    return generate_pool(n, depth, nullptr, 0, &c, weighted);
+}
+
+int nqb_generate_pool(unsigned n, unsigned depth, nqb_state** states, uint64_t* count) {
+    if (!states || !count) return NQB_E_INVALID;
+    *states = nullptr;
+    uint64_t c = 0;
+    NQB_TRY(generate_pool(n, depth, nullptr, 0, &c, nullptr));
+    nqb_state* p = static_cast<nqb_state*>(aligned_host_alloc(c * sizeof(nqb_state)));
+    if (!p) return NQB_E_NOMEM;
+    const int s = generate_pool(n, depth, p, c, count, nullptr);
+    if (s != NQB_OK) {
+        std::free(p);
+        return s;
+    }
+    *states = p;
+    return NQB_OK;
+}
+
+int nqb_count_ex(unsigned n, unsigned depth, const nqb_opts* opts, uint64_t* count, nqb_stats* stats) {
+    const double t0 = now_ms();
+    if (!count || n < NQB_MIN_N || n > NQB_MAX_N || depth < 1 || depth >= n) return NQB_E_INVALID;
+    const nqb_opts o = resolve(opts);
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    Scope sc(o.device);
+    NQB_TRY(sc.status);
+    nqb_state* pool = nullptr;
+    uint64_t cnt = 0;
+    const double tg = now_ms();
+    NQB_TRY(nqb_generate_pool(n, depth, &pool, &cnt));
+    const double gen_ms = now_ms() - tg;
+    unsigned long long totals[4] = {0, 0, 0, 0};
+    const int s = solve_host_states(sc, pool, cnt, o, totals, nullptr, stats);
+    std::free(pool);
+    NQB_TRY(s);
+    *count = totals[0];
+    if (stats) {
+        stats->gen_ms = gen_ms;
+        stats->pregen_depth = depth;
+        stats->wall_ms = now_ms() - t0;
+    }
+    return NQB_OK;
+}
+
+int nqb_count(unsigned n, unsigned depth, uint64_t* count) { return nqb_count_ex(n, depth, nullptr, count, nullptr); }
+
+int nqb_solve_states(const nqb_state* states, uint64_t count, const nqb_opts* opts, uint64_t* total,
+                     nqb_stats* stats) {
+    const double t0 = now_ms();
+    if (!total || (count && !states)) return NQB_E_INVALID;
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    *total = 0;
+    if (count == 0) return NQB_OK;
+    const nqb_opts o = resolve(opts);
+    Scope sc(o.device);
+    NQB_TRY(sc.status);
+    unsigned long long totals[4] = {0, 0, 0, 0};
+    NQB_TRY(solve_host_states(sc, states, count, o, totals, nullptr, stats));
+    *total = totals[0];
+    if (stats) stats->wall_ms = now_ms() - t0;
+    return NQB_OK;
+}
+
+int nqb_solve_batch(const nqb_state* boards, uint64_t count, const nqb_opts* opts, uint64_t* out,
+                    nqb_stats* stats) {
+    const double t0 = now_ms();
+    if (!out || (count && !boards)) return NQB_E_INVALID;
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    if (count == 0) return NQB_OK;
+    const nqb_opts o = resolve(opts);
+    Scope sc(o.device);
+    NQB_TRY(sc.status);
+    unsigned long long totals[4] = {0, 0, 0, 0};
+    NQB_TRY(solve_host_states(sc, boards, count, o, totals, out, stats));
+    if (stats) stats->wall_ms = now_ms() - t0;
+    return NQB_OK;
+}
+
+size_t nqb_ref_state_size(unsigned n) {
+    if (n < 1 || n > NQB_MAX_N) return 0;
+    return ((16u + 4u + 1u + n) + 7u) & ~(size_t)7u;
+}
+
+int nqb_states_from_ref(unsigned n, const void* ref_states, uint64_t count, int mirror_weight, nqb_state* out) {
+    if (n < NQB_MIN_N || n > NQB_MAX_N || (count && (!ref_states || !out))) return NQB_E_INVALID;
+    const size_t sz = nqb_ref_state_size(n);
+    const uint8_t* p = static_cast<const uint8_t*>(ref_states);
+    const uint32_t mask = board_mask(n);
+    for (uint64_t i = 0; i < count; ++i, p += sz) {
+        uint64_t diag, anti;
+        uint32_t cols;
+        std::memcpy(&diag, p, 8);
+        std::memcpy(&anti, p + 8, 8);
+        std::memcpy(&cols, p + 16, 4);
+        const int row = (int8_t)p[20];
+        if (row < 0 || row > (int)n || (cols & ~mask)) return NQB_E_INVALID;
+        nqb_state& s = out[i];
+        s.cols = cols;
+        s.rdiag = (uint32_t)(diag >> row);                 // diagonals.cuh:17-20
+        s.ldiag = (uint32_t)(anti >> (n - (unsigned)row));
+        s.row = (uint8_t)row;
+        s.n = (uint8_t)n;
+        s.weight = (uint8_t)(mirror_weight ? (p[21] < (n >> 1) ? 2 : 1) : 1);  // GPU_NQueens.cu:356
+        s.flags = 0;
+    }
+    return NQB_OK;
+}
+
+int nqb_solve_ref_states(unsigned n, const void* ref_states, uint64_t count, unsigned locked_row,
+                         const nqb_opts* opts, uint64_t* total) {
+    if (!total || n < NQB_MIN_N || n > NQB_MAX_N || locked_row < 1 || locked_row >= n) return NQB_E_INVALID;
+    if (count && !ref_states) return NQB_E_INVALID;
+    *total = 0;
+    if (count == 0) return NQB_OK;
+    nqb_state* st = static_cast<nqb_state*>(aligned_host_alloc(count * sizeof(nqb_state)));
+    if (!st) return NQB_E_NOMEM;
+    int s = nqb_states_from_ref(n, ref_states, count, 1, st);
+    for (uint64_t i = 0; s == NQB_OK && i < count; ++i)
+        if (st[i].row != locked_row) s = NQB_E_INVALID;  // the reference solves one lock row per call
+    if (s == NQB_OK) s = nqb_solve_states(st, count, opts, total, nullptr);
+    std::free(st);
+    return s;
+}
+
+int nqb_plain_launch(const nqb_state* d_states, uint64_t count, uint64_t* d_out, int block_size,
+                     int count_unit_nodes, unsigned stack_depth, void* stream) {
+    return launch_plain(d_states, count, reinterpret_cast<unsigned long long*>(d_out), nullptr, block_size,
+                        count_unit_nodes != 0, stack_depth, static_cast<cudaStream_t>(stream), nullptr);
+}
+
+}  // extern "C"

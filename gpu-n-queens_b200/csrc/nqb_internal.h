@@ -1,0 +1,34 @@
+// Internal declarations shared by the translation units of libnqb.so.
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "nqb.h"
+
+namespace nqb {
+
+inline uint32_t board_mask(unsigned n) { return n >= 32 ? 0xFFFFFFFFu : ((1u << n) - 1u); }
+
+// Host pool generator (pool.cpp).  With buf == nullptr only count/weighted are computed.
+// Returns NQB_E_RANGE when the pool holds more than `capacity` states.
+int generate_pool(unsigned n, unsigned depth, nqb_state* buf, uint64_t capacity, uint64_t* count,
+                  uint64_t* weighted);
+
+// Worker threads used by host-side passes (NQB_THREADS overrides the core count).
+unsigned host_threads();
+
+// Largest number of free columns minus one over `count` states: the deepest stack of
+// pending alternatives one search can hold.
+unsigned max_stack_depth(const nqb_state* states, uint64_t count);
+
+// Plain search kernel (plain.cu).  d_out: {weighted count, nodes, unit nodes, error flags}.
+// d_per_state (optional): weight x completions per state.
+int launch_plain(const nqb_state* d_states, uint64_t count, unsigned long long* d_out,
+                 unsigned long long* d_per_state, int block_size, bool count_unit, unsigned stack_depth,
+                 cudaStream_t stream, unsigned* launches);
+
+int cuda_status(cudaError_t e);
+
+}  // namespace nqb

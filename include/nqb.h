@@ -1,0 +1,213 @@
+/*
+ * nqb.h - C ABI of the B200 N-Queens counter (libnqb.so).
+ *
+ * The library counts N-Queens solutions with the DoubleSweep-light search of
+ * fillpant/GPU-N-Queens: a host-built pool of every valid placement of the first
+ * `depth` rows (row 0 restricted to the left half of the board, counts of
+ * left-half states doubled), then one depth-first search per pool state with
+ * unit-row propagation, summed into a uint64 count.
+ *
+ * Every entry point returns an NQB_* status code and never exits the process
+ * (the reference's FAIL_IF / CHECK_CUDA_ERROR exit; deffinitions.cuh:148-156).
+ * Plain pointers and sizes only; no C++ or torch types cross this boundary.
+ * Calls are re-entrant: each call owns its own stream and device buffers.
+ */
+#ifndef NQB_H
+#define NQB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NQB_VERSION 10000 /* 1.0.0 */
+
+/* Board sizes.  The reference accepts 7 < N < 32 (deffinitions.cuh:116-118);
+ * this library accepts 4..31.  Counts are exact in uint64 up to N = 28. */
+#define NQB_MIN_N 4
+#define NQB_MAX_N 31
+
+/* ---- status codes ------------------------------------------------------ */
+#define NQB_OK 0
+#define NQB_E_INVALID 1  /* bad argument: n, depth, null pointer, bad state      */
+#define NQB_E_NOMEM 2    /* host allocation failed (reference: errno ENOMEM)      */
+#define NQB_E_CUDA 3     /* CUDA runtime error (reference: CHECK_CUDA_ERROR exit) */
+#define NQB_E_NODEVICE 4 /* no usable sm_100 device (reference: check_gpu_compatibility) */
+#define NQB_E_RANGE 5    /* size beyond a supported limit (reference: errno ERANGE) */
+#define NQB_E_STALL 6    /* a device-side bounded wait ran out                    */
+#define NQB_E_DEVICE 7   /* a device-side bounds check failed                     */
+#define NQB_E_MODEL 8    /* learned cost model missing or not trained            */
+
+/* ---- search state ------------------------------------------------------ */
+/*
+ * One search state: rows [0, row) hold queens, the search continues at `row`.
+ * 16 bytes, the unit of the pool in host memory and in HBM.
+ *
+ *   cols   bit c set <=> a queen stands in column c
+ *   ldiag  bit c set <=> column c of row `row` is attacked along a diagonal
+ *          whose column grows with the row (each row down shifts it left 1)
+ *   rdiag  same for diagonals whose column shrinks with the row (shift right 1)
+ *   weight multiplier applied to this state's completion count: 2 for a row-0
+ *          queen in the left half (column < n/2), 1 for the middle column of an
+ *          odd board, 1 for arbitrary boards solved without mirror weighting
+ *
+ * Relation to the reference's nq_state_t (n_queens.cuh:100-113; diagonals.cuh:8-34)
+ * at curr_row = r:  cols = queens_in_columns,
+ *   rdiag = (uint32)(diagonal >> r),  ldiag = (uint32)(antidiagonal >> (N - r)).
+ */
+typedef struct nqb_state {
+    uint32_t cols;
+    uint32_t ldiag;
+    uint32_t rdiag;
+    uint8_t row;
+    uint8_t n;
+    uint8_t weight;
+    uint8_t flags; /* reserved, must be 0 */
+} nqb_state;
+
+/* ---- options and statistics ------------------------------------------- */
+#define NQB_FORM_PLAIN 0   /* one thread per state, static assignment            */
+#define NQB_FORM_BATCHED 1 /* persistent kernel, device work queue, re-splitting */
+
+typedef struct nqb_opts {
+    int device;           /* CUDA device ordinal (default 0)                           */
+    int form;             /* NQB_FORM_PLAIN or NQB_FORM_BATCHED                        */
+    int block_size;       /* threads per block; 0 = library default                    */
+    int count_unit_nodes; /* 1: also count unit-propagation placements (slower kernel) */
+    int use_model;        /* batched form: 1 = order/split with the learned model      */
+    int split_depth;      /* batched form: extra rows pre-expanded for large states;
+                             -1 = library default                                       */
+    int reserved[10];
+} nqb_opts;
+
+typedef struct nqb_stats {
+    uint64_t states;     /* pool states (or boards) solved                         */
+    uint64_t nodes;      /* queen placements at rows >= each state's start row     */
+    uint64_t unit_nodes; /* of which unit-row propagations; UINT64_MAX if not counted */
+    double gen_ms;       /* host pool generation                                   */
+    double h2d_ms;       /* host->device copy of the pool                          */
+    double kernel_ms;    /* device time of the search kernels (CUDA events)        */
+    double wall_ms;      /* whole call                                             */
+    uint32_t pregen_depth;
+    uint32_t kernel_launches;
+    uint32_t reserved[6];
+} nqb_stats;
+
+/* Fills `opts` with the defaults (device 0, plain form, library block size). */
+void nqb_default_opts(nqb_opts* opts);
+
+/* Human-readable text for a status code (static storage). */
+const char* nqb_strerror(int status);
+
+int nqb_version(void);
+
+/* Checks that `device` is an sm_100 GPU this library can run on.
+ * Replaces check_gpu_compatibility (GPU_NQueens.cu:23-54). */
+int nqb_device_check(int device);
+
+/* ---- the drop-in count -------------------------------------------------- */
+/*
+ * Counts all solutions of the n-queens puzzle: builds the pool of every valid
+ * `pregen_depth`-row prefix (row-0 queen in columns < ceil(n/2), prefixes whose
+ * next row has no free column dropped), solves it on the GPU and returns the
+ * mirror-weighted uint64 total.  1 <= pregen_depth <= n-1.
+ * Replaces nq_generate_states_rowlock (n_queens.cuh:119) followed by
+ * solve() / gpu_solver_driver (NQ_solver.cu:192-209, GPU_NQueens.cuh:13).
+ */
+int nqb_count(unsigned n, unsigned pregen_depth, uint64_t* count);
+
+/* nqb_count with options (NULL = defaults) and statistics (may be NULL). */
+int nqb_count_ex(unsigned n, unsigned pregen_depth, const nqb_opts* opts, uint64_t* count,
+                 nqb_stats* stats);
+
+/* ---- the pool ----------------------------------------------------------- */
+/*
+ * Builds the pool on the host: the same prefixes, in the same order, as the
+ * reference's gen_states_threaded_rowlock (n_queens.cu:235-315): row-0 columns
+ * 0..ceil(n/2)-1 in turn, each followed by its prefixes in depth-first order,
+ * lowest column first.  *states is allocated by the library (16-byte aligned);
+ * release it with nqb_free.  Replaces nq_generate_states_rowlock (n_queens.cuh:119).
+ */
+int nqb_generate_pool(unsigned n, unsigned depth, nqb_state** states, uint64_t* count);
+
+/* Same, into a caller buffer of `capacity` states.  With buf == NULL only the
+ * size is computed.  Returns NQB_E_RANGE if the pool does not fit. */
+int nqb_generate_pool_into(unsigned n, unsigned depth, nqb_state* buf, uint64_t capacity,
+                           uint64_t* count);
+
+/* Sum of the pool's weights: the number of full-board prefixes it stands for. */
+int nqb_pool_weighted_size(unsigned n, unsigned depth, uint64_t* weighted);
+
+void nqb_free(void* p);
+
+/*
+ * Seeded random valid partial boards (no counterpart in the reference, which has no
+ * batch mode): board i draws n uniformly from [n_min, n_max] and a depth uniformly
+ * from [d_min, d_max], then fills rows 0..depth-1 in order, each with a column drawn
+ * uniformly among the row's free columns, restarting the board when a row before the
+ * depth has no free column.  Row `depth` may be dead (the board then has 0
+ * completions).  Weight 1.  Random stream: splitmix64 from `seed`; a draw in [0, k)
+ * is ((next >> 32) * k) >> 32.
+ */
+int nqb_sample_boards(uint64_t seed, uint64_t count, unsigned n_min, unsigned n_max, unsigned d_min,
+                      unsigned d_max, nqb_state* out);
+
+/* ---- solving states ---------------------------------------------------- */
+/*
+ * Solves `count` states held in host memory on the GPU and returns the sum of
+ * weight x completions.  States may mix board sizes and start rows.
+ * Replaces gpu_solver_driver (GPU_NQueens.cuh:13) for the library's state layout.
+ */
+int nqb_solve_states(const nqb_state* states, uint64_t count, const nqb_opts* opts,
+                     uint64_t* total, nqb_stats* stats);
+
+/*
+ * Per-board completion counts: out[i] = weight_i x completions of boards[i]
+ * (pass weight 1 for plain counts; no mirror weighting is implied).
+ * Boards may mix n (4..31) and row.  Used for batches of uneven partial boards.
+ */
+int nqb_solve_batch(const nqb_state* boards, uint64_t count, const nqb_opts* opts,
+                    uint64_t* out, nqb_stats* stats);
+
+/* Size in bytes of the reference's nq_state_t for board size n
+ * ({u64 diagonal, u64 antidiagonal, u32 cols, char curr_row, u8 queen_at_index[n]},
+ * 8-byte aligned; n_queens.cuh:100-113). */
+size_t nqb_ref_state_size(unsigned n);
+
+/*
+ * Converts `count` reference nq_state_t records (stride nqb_ref_state_size(n)) to
+ * library states.  With mirror_weight != 0 the weight is 2 when queen_at_index[0]
+ * < n/2, else 1 (GPU_NQueens.cu:354-357,437-439); otherwise 1.
+ */
+int nqb_states_from_ref(unsigned n, const void* ref_states, uint64_t count, int mirror_weight,
+                        nqb_state* out);
+
+/*
+ * Direct replacement for gpu_solver_driver (GPU_NQueens.cu:56-175) on a buffer of
+ * reference nq_state_t records generated for lock row `locked_row` (every state
+ * has curr_row == locked_row): mirror-weighted total in *total.
+ */
+int nqb_solve_ref_states(unsigned n, const void* ref_states, uint64_t count, unsigned locked_row,
+                         const nqb_opts* opts, uint64_t* total);
+
+/* ---- device-resident launches (inputs already in HBM) ------------------- */
+/*
+ * Plain form on states already in device memory: one thread per state.
+ * d_out points to 4 device uint64 words {weighted count, nodes, unit nodes, error
+ * flags}; the kernel adds into them, so zero them first.  Unit nodes are counted
+ * only with count_unit_nodes != 0.  stack_depth bounds the pending rows one search
+ * can hold: the largest number of free columns of any state minus one (0 = 30);
+ * a search that needs more sets error flag 1 in d_out[3].  `stream` is a
+ * cudaStream_t (NULL = legacy default stream).  Asynchronous: returns after the
+ * launch.  The kernel launch of gpu_solver_driver (GPU_NQueens.cu:128-138).
+ */
+int nqb_plain_launch(const nqb_state* d_states, uint64_t count, uint64_t* d_out, int block_size,
+                     int count_unit_nodes, unsigned stack_depth, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NQB_H */
