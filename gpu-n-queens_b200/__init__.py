@@ -93,6 +93,8 @@ def lib():
                                                  ctypes.c_uint, ctypes.c_uint, vp]),
             "nqb_plain_launch": (ctypes.c_int, [vp, ctypes.c_uint64, vp, ctypes.c_int, ctypes.c_int,
                                                 ctypes.c_uint, vp]),
+            "nqb_batched_launch": (ctypes.c_int, [vp, ctypes.c_uint64, vp, vp, vp, ctypes.c_int, ctypes.c_uint,
+                                                  vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -239,6 +241,13 @@ def plain_launch(d_states_ptr, count, d_out_ptr, block_size=0, count_unit_nodes=
     """Launches the plain kernel on device pointers (see nqb_plain_launch)."""
     _check(lib().nqb_plain_launch(d_states_ptr, count, d_out_ptr, block_size, int(count_unit_nodes),
                                   stack_depth, stream or None), "nqb_plain_launch")
+
+
+def batched_launch(d_items_ptr, count, d_head_ptr, d_out_ptr, d_order_ptr=None, block_size=0, stack_depth=0,
+                   stream=0):
+    """Launches the batched (persistent, work-queue) kernel on device pointers."""
+    _check(lib().nqb_batched_launch(d_items_ptr, count, d_order_ptr, d_head_ptr, d_out_ptr, block_size,
+                                    stack_depth, stream or None), "nqb_batched_launch")
 
 
 def header_symbols():

@@ -30,13 +30,14 @@ double now_ms() {
 class Scope {
    public:
     int status = NQB_OK;
+    int device = 0;
     cudaStream_t stream = nullptr;
 
-    explicit Scope(int device) {
+    explicit Scope(int dev) : device(dev) {
         cudaGetDevice(&prev_);
-        status = nqb_device_check(device);
+        status = nqb_device_check(dev);
         if (status != NQB_OK) return;
-        if ((status = cuda_status(cudaSetDevice(device))) != NQB_OK) return;
+        if ((status = cuda_status(cudaSetDevice(dev))) != NQB_OK) return;
         status = cuda_status(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     }
     ~Scope() {
@@ -87,19 +88,23 @@ bool state_ok(const nqb_state& s) {
     return (s.cols & ~board_mask(s.n)) == 0;
 }
 
-// Solves `count` host states on the device; fills totals {count, nodes, unit, err}
-// and, if per_state != nullptr, per-state weighted counts.
+// Solves `count` host states on the device with the form o.form; fills totals
+// {count, nodes, unit, err} and, if per_state != nullptr, per-state weighted counts.
 int solve_host_states(Scope& sc, const nqb_state* states, uint64_t count, const nqb_opts& o,
                       unsigned long long totals[4], uint64_t* per_state, nqb_stats* st) {
     for (uint64_t i = 0; i < count; ++i)
         if (!state_ok(states[i])) return NQB_E_INVALID;
+    const bool batched = o.form == NQB_FORM_BATCHED;
+    if (o.form != NQB_FORM_PLAIN && !batched) return NQB_E_INVALID;
+    if (batched && count > (1ull << 31)) return NQB_E_RANGE;
     const unsigned depth = max_stack_depth(states, count);
     nqb_state* d_states = nullptr;
-    unsigned long long* d_out = nullptr;
+    unsigned long long* d_out = nullptr;  // 4 result words, then the queue head
     unsigned long long* d_per = nullptr;
     NQB_TRY(sc.alloc(&d_states, count * sizeof(nqb_state)));
-    NQB_TRY(sc.alloc(&d_out, 4 * sizeof(unsigned long long)));
+    NQB_TRY(sc.alloc(&d_out, 5 * sizeof(unsigned long long)));
     if (per_state) NQB_TRY(sc.alloc(&d_per, count * sizeof(unsigned long long)));
+    uint32_t* d_head = reinterpret_cast<uint32_t*>(d_out + 4);
     cudaEvent_t e0, e1, e2;
     NQB_TRY(sc.event(&e0));
     NQB_TRY(sc.event(&e1));
@@ -107,11 +112,17 @@ int solve_host_states(Scope& sc, const nqb_state* states, uint64_t count, const 
     NQB_TRY(cuda_status(cudaEventRecord(e0, sc.stream)));
     NQB_TRY(cuda_status(
         cudaMemcpyAsync(d_states, states, count * sizeof(nqb_state), cudaMemcpyHostToDevice, sc.stream)));
-    NQB_TRY(cuda_status(cudaMemsetAsync(d_out, 0, 4 * sizeof(unsigned long long), sc.stream)));
+    NQB_TRY(cuda_status(cudaMemsetAsync(d_out, 0, 5 * sizeof(unsigned long long), sc.stream)));
+    if (d_per) NQB_TRY(cuda_status(cudaMemsetAsync(d_per, 0, count * sizeof(unsigned long long), sc.stream)));
     NQB_TRY(cuda_status(cudaEventRecord(e1, sc.stream)));
     unsigned launches = 0;
-    NQB_TRY(launch_plain(d_states, count, d_out, d_per, o.block_size, o.count_unit_nodes != 0, depth, sc.stream,
-                         &launches));
+    if (batched) {
+        NQB_TRY(launch_batched(d_states, (uint32_t)count, nullptr, nullptr, d_head, d_out, d_per, nullptr,
+                               o.block_size, depth, sc.device, sc.stream, &launches));
+    } else {
+        NQB_TRY(launch_plain(d_states, count, d_out, d_per, o.block_size, o.count_unit_nodes != 0, depth,
+                             sc.stream, &launches));
+    }
     NQB_TRY(cuda_status(cudaEventRecord(e2, sc.stream)));
     NQB_TRY(cuda_status(cudaMemcpyAsync(totals, d_out, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                                         sc.stream)));
@@ -126,7 +137,7 @@ int solve_host_states(Scope& sc, const nqb_state* states, uint64_t count, const 
         cudaEventElapsedTime(&ker, e1, e2);
         st->states = count;
         st->nodes = totals[1];
-        st->unit_nodes = o.count_unit_nodes ? totals[2] : UINT64_MAX;
+        st->unit_nodes = (o.count_unit_nodes && !batched) ? totals[2] : UINT64_MAX;
         st->h2d_ms = h2d;
         st->kernel_ms = ker;
         st->kernel_launches = launches;
@@ -324,6 +335,16 @@ int nqb_plain_launch(const nqb_state* d_states, uint64_t count, uint64_t* d_out,
                      int count_unit_nodes, unsigned stack_depth, void* stream) {
     return launch_plain(d_states, count, reinterpret_cast<unsigned long long*>(d_out), nullptr, block_size,
                         count_unit_nodes != 0, stack_depth, static_cast<cudaStream_t>(stream), nullptr);
+}
+
+int nqb_batched_launch(const nqb_state* d_items, uint64_t count, const uint32_t* d_order, uint32_t* d_head,
+                       uint64_t* d_out, int block_size, unsigned stack_depth, void* stream) {
+    if (count > (1ull << 31)) return NQB_E_RANGE;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return NQB_E_NODEVICE;
+    return launch_batched(d_items, (uint32_t)count, d_order, nullptr, d_head,
+                          reinterpret_cast<unsigned long long*>(d_out), nullptr, nullptr, block_size, stack_depth, dev,
+                          static_cast<cudaStream_t>(stream), nullptr);
 }
 
 }  // extern "C"

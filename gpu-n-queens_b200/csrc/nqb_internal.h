@@ -29,6 +29,14 @@ int launch_plain(const nqb_state* d_states, uint64_t count, unsigned long long* 
                  unsigned long long* d_per_state, int block_size, bool count_unit, unsigned stack_depth,
                  cudaStream_t stream, unsigned* launches);
 
+// Batched (persistent, work-queue) search kernel (batched.cu).  d_head: queue head,
+// zeroed before launch.  d_order (optional): queue position -> item; d_board_of
+// (optional): item -> output slot.  d_out: {weighted count, nodes, 0, error flags}.
+int launch_batched(const nqb_state* d_items, uint32_t n_items, const uint32_t* d_order, const uint32_t* d_board_of,
+                   uint32_t* d_head, unsigned long long* d_out, unsigned long long* d_per_board,
+                   unsigned long long* d_per_board_nodes, int block_size, unsigned stack_depth, int device,
+                   cudaStream_t stream, unsigned* launches);
+
 int cuda_status(cudaError_t e);
 
 }  // namespace nqb

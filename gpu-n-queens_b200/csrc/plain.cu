@@ -1,118 +1,91 @@
 // Plain form: one thread per pool state, the drop-in for kern_doitall_v2_regld
 // (GPU_NQueens.cu:338-452) and its launch in gpu_solver_driver (GPU_NQueens.cu:128-138).
 //
-// Each thread runs a depth-first search from its state.  Per row the thread keeps
-// four 32-bit words in registers:
-//   avail  candidate columns of the current row not tried yet
-//   nc     columns still without a queen
-//   l, r   columns of the current row attacked along the two diagonals
-// One loop iteration places exactly one queen (one search node):
-//   - when avail is empty it pops the deepest row that still has candidates from a
-//     per-thread stack in shared memory (16 bytes per entry, one LDS.128),
-//   - it takes the lowest candidate b, and pushes the row back (one STS.128) only if
-//     candidates remain,
-//   - it steps to the next row: nc ^= b, l = (l|b) << 1, r = (r|b) >> 1,
-//     avail = nc & ~(l|r).
-// A row that is left with no candidate is never pushed, so a row with exactly one
-// free column is filled and passed through without a branch point: that is the
-// reference's DoubleSweep-light unit-row propagation (GPU_NQueens.cu:392-408), and
-// the set of placements (nodes) equals the reference's.  nc == 0 marks a solution
-// (the reference tests cols == N_MASK, GPU_NQueens.cu:420-424).
-// The warp leaves the loop by a __any_sync vote when every lane is done
-// (GPU_NQueens.cu:358-360).  Counts are reduced per warp with shuffles and per
-// block through shared memory, then added with one uint64 atomic per block.
+// Each thread runs the depth-first search of search_step.cuh from its state; the
+// warp leaves the loop by a __all_sync vote once every lane is parked
+// (GPU_NQueens.cu:358-360).  kUnroll steps run between votes; a lane that finishes in
+// between stays parked.  Counters are 32-bit per lane and are folded into 64-bit
+// totals every kEpoch votes, so no lane counter can wrap.  Counts are reduced per warp
+// with shuffles and per block through shared memory, then added with one uint64
+// atomic per block (the reference adds one atomic per thread, GPU_NQueens.cu:441-443).
 #include <algorithm>
 
 #include "nqb_internal.h"
+#include "search_step.cuh"
 
 namespace nqb {
 namespace {
 
 constexpr unsigned kFull = 0xFFFFFFFFu;
-
-__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFull, v, o);
-    return v;
-}
+constexpr int kUnroll = 16;
+constexpr uint32_t kEpoch = 1u << 27;  // votes between folds: kUnroll x kEpoch < 2^32
 
 // Error flags written to out[3].
-constexpr unsigned long long kErrStack = 1ull;  // a search needed more stack than provided
+constexpr unsigned long long kErrStack = 1ull;  // a state needed a deeper stack than provided
 
 // per_state (optional): weight x completions of each state, for per-board results.
+// UNIT: also count placements made by unit-row propagation (the reference's split of
+// nodes; a row entered with exactly one free column, other than the start row).
 template <int BLOCK, bool UNIT>
 __global__ void __launch_bounds__(BLOCK) plain_search_kernel(const uint4* __restrict__ states, uint32_t count,
                                                              unsigned long long* __restrict__ out,
                                                              unsigned long long* __restrict__ per_state,
                                                              uint32_t stack_depth) {
-    extern __shared__ uint4 stack[];  // [stack_depth][BLOCK]
+    extern __shared__ uint4 stack[];  // [stack_depth + 1][BLOCK]; row 0 holds the sentinels
+    constexpr int kStride = BLOCK * 16;
     const uint32_t tid = threadIdx.x;
     const uint32_t gi = blockIdx.x * BLOCK + tid;
+    const uint32_t base = (uint32_t)__cvta_generic_to_shared(stack) + tid * 16;
+    write_sentinel(base);
 
-    uint32_t avail = 0, nc = 0, l = 0, r = 0, weight = 0;
+    Lane s;
+    lane_park(s, base);
+    s.sols = 0;
+    s.nodes = 0;
+    uint32_t weight = 0;
+    bool bad = false;
+    if (gi < count) {
+        const uint4 st = __ldg(states + gi);
+        weight = (st.w >> 16) & 0xFFu;
+        if (lane_load(s, st, base) > stack_depth) {
+            bad = true;
+            lane_park(s, base);
+            s.sols = 0;
+        }
+    }
     unsigned long long sols = 0, nodes = 0;
     uint32_t unit = 0;
     bool first = true;
-    if (gi < count) {
-        const uint4 s = __ldg(states + gi);
-        const uint32_t n = (s.w >> 8) & 0xFFu;
-        const uint32_t mask = n >= 32 ? kFull : ((1u << n) - 1u);
-        nc = mask & ~s.x;
-        l = s.y;
-        r = s.z;
-        weight = (s.w >> 16) & 0xFFu;
-        avail = nc & ~(l | r);
-        sols = (nc == 0);  // a complete board handed in as a state
-    }
-    uint32_t sp = tid;  // next free stack slot; the stack base is tid
-    const uint32_t sp_lim = tid + stack_depth * BLOCK;
-    bool overflow = false;
-
     for (;;) {
-        const bool active = (avail != 0) | (sp != tid);
-        if (!__any_sync(kFull, active)) break;
-        if (active) {
-            bool fresh = !first;
-            if (avail == 0) {  // backtrack to the deepest row with candidates left
-                sp -= BLOCK;
-                const uint4 e = stack[sp];
-                avail = e.x;
-                nc = e.y;
-                l = e.z;
-                r = e.w;
-                fresh = false;
+        bool done = false;
+        for (uint32_t v = 0; v < kEpoch; ++v) {
+            if (__all_sync(kFull, s.avail == 0 && s.sp == base)) {
+                done = true;
+                break;
             }
-            const uint32_t b = avail & (0u - avail);
-            if (UNIT) unit += (fresh && avail == b);  // row entered with one free column
-            first = false;
-            avail ^= b;
-            if (avail) {
-                if (sp < sp_lim) {
-                    stack[sp] = make_uint4(avail, nc, l, r);
-                    sp += BLOCK;
-                } else {  // cannot happen when stack_depth covers the states; flag it
-                    overflow = true;
-                    avail = 0;
-                    sp = tid;
+#pragma unroll
+            for (int u = 0; u < kUnroll; ++u) {
+                if (UNIT) {
+                    unit += (!first && s.avail != 0 && (s.avail & (s.avail - 1u)) == 0);
+                    first = false;
                 }
+                search_step<kStride>(s, base);
             }
-            nc ^= b;
-            l = (l | b) << 1;
-            r = (r | b) >> 1;
-            avail = nc & ~(l | r);
-            sols += (nc == 0);
-            nodes++;
         }
+        sols += s.sols;
+        nodes += s.nodes;
+        s.sols = 0;
+        s.nodes = 0;
+        if (done) break;
     }
 
     unsigned long long c = sols * weight;
     if (per_state && gi < count) per_state[gi] = c;
-    unsigned long long nd = nodes;
     unsigned long long un = unit;
     c = warp_sum_u64(c);
-    nd = warp_sum_u64(nd);
+    nodes = warp_sum_u64(nodes);
     if (UNIT) un = warp_sum_u64(un);
-    const unsigned any_overflow = __any_sync(kFull, overflow);
+    const unsigned any_bad = __any_sync(kFull, bad);
 
     __syncthreads();  // the stack area is reused for the block reduction
     unsigned long long* red = reinterpret_cast<unsigned long long*>(stack);
@@ -120,23 +93,23 @@ __global__ void __launch_bounds__(BLOCK) plain_search_kernel(const uint4* __rest
     constexpr int kWarps = BLOCK / 32;
     if (lane == 0) {
         red[warp] = c;
-        red[kWarps + warp] = nd;
+        red[kWarps + warp] = nodes;
         red[2 * kWarps + warp] = un;
-        red[3 * kWarps + warp] = any_overflow;
+        red[3 * kWarps + warp] = any_bad;
     }
     __syncthreads();
     if (warp == 0) {
         c = lane < kWarps ? red[lane] : 0;
-        nd = lane < kWarps ? red[kWarps + lane] : 0;
+        nodes = lane < kWarps ? red[kWarps + lane] : 0;
         un = lane < kWarps ? red[2 * kWarps + lane] : 0;
         unsigned long long of = lane < kWarps ? red[3 * kWarps + lane] : 0;
         c = warp_sum_u64(c);
-        nd = warp_sum_u64(nd);
+        nodes = warp_sum_u64(nodes);
         un = warp_sum_u64(un);
         of = warp_sum_u64(of);
         if (lane == 0) {
             if (c) atomicAdd(out + 0, c);
-            atomicAdd(out + 1, nd);
+            atomicAdd(out + 1, nodes);
             if (UNIT && un) atomicAdd(out + 2, un);
             if (of) atomicOr(out + 3, kErrStack);
         }
@@ -147,8 +120,8 @@ template <int BLOCK, bool UNIT>
 int launch_t(const nqb_state* d_states, uint64_t count, unsigned long long* d_out,
              unsigned long long* d_per_state, unsigned stack_depth, cudaStream_t stream, unsigned* launches) {
     auto kern = plain_search_kernel<BLOCK, UNIT>;
-    // Room for the stack, and for 4 x (BLOCK/32) reduction words.
-    const size_t smem = std::max<size_t>((size_t)stack_depth * BLOCK * sizeof(uint4),
+    // Room for the stack (with its sentinel row), and for 4 x (BLOCK/32) reduction words.
+    const size_t smem = std::max<size_t>((size_t)(stack_depth + 1) * BLOCK * sizeof(uint4),
                                          4 * (BLOCK / 32) * sizeof(unsigned long long));
     if (smem > 227 * 1024) return NQB_E_RANGE;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -206,6 +206,17 @@ int nqb_solve_ref_states(unsigned n, const void* ref_states, uint64_t count, uns
 int nqb_plain_launch(const nqb_state* d_states, uint64_t count, uint64_t* d_out, int block_size,
                      int count_unit_nodes, unsigned stack_depth, void* stream);
 
+/*
+ * Batched form on items already in device memory: a persistent kernel (one wave of
+ * blocks over all SMs of the current device) that hands items to idle lanes from a
+ * queue and, once the queue is empty, splits the pending rows of busy lanes onto
+ * idle ones.  d_order (optional) gives the queue order as item indices; d_head is a
+ * device uint32 queue head (scratch) that must be zero at launch; d_out as for
+ * nqb_plain_launch (unit nodes are not counted).  count <= 2^31.  Asynchronous.
+ */
+int nqb_batched_launch(const nqb_state* d_items, uint64_t count, const uint32_t* d_order, uint32_t* d_head,
+                       uint64_t* d_out, int block_size, unsigned stack_depth, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
