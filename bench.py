@@ -31,6 +31,11 @@ sys.path.insert(0, ROOT)
 
 KAT = {13: 73712, 17: 95815104, 18: 666090624, 19: 4968057848, 20: 39029188884, 21: 314666222712,
        22: 2691008701644}
+# Search nodes of full counts: (17, 5) and (18, 6) equal the reference's own kernel-loop
+# replay (tests/golden); the others are the counts both kernel forms report, which the
+# GPU tests pin on stride samples of each pool against the reference replay.
+NODES = {(17, 5): 4275902721, (18, 6): 29681542262, (19, 7): 245072203329, (20, 7): 1884962763151,
+         (21, 7): 16976718185320}
 INT_OPS_PER_NODE = 15  # algorithmic INT32 lane-ops per node (fixed convention)
 METRIC = "N=21 count wall-time & nodes/s on 1 GPU: batched+learned vs plain, bit-exact"
 
@@ -158,15 +163,25 @@ def run_nqb(args):
     stack_depth = n - d - 1
     d_pool = torch.from_numpy(pool.view(np.uint8)).to(f"cuda:{dev}")
     d_out = torch.zeros((max(args.steps, args.warmup), 4), dtype=torch.int64, device=f"cuda:{dev}")
+    d_head = torch.zeros(max(args.steps, args.warmup), dtype=torch.int32, device=f"cuda:{dev}")
     stream = torch.cuda.current_stream(dev)
     sptr = stream.cuda_stream
+    form = {"plain": nqb.FORM_PLAIN, "batched": nqb.FORM_BATCHED}[args.form]
+
+    def launch(f, out_row, head_slot):
+        if f == nqb.FORM_PLAIN:
+            nqb.plain_launch(d_pool.data_ptr(), states, out_row.data_ptr(), block_size=args.block,
+                             stack_depth=stack_depth, stream=sptr)
+        else:
+            nqb.batched_launch(d_pool.data_ptr(), states, head_slot.data_ptr(), out_row.data_ptr(),
+                               block_size=args.block, stack_depth=stack_depth, stream=sptr)
 
     def step(i):
-        nqb.plain_launch(d_pool.data_ptr(), states, d_out[i].data_ptr(), block_size=args.block,
-                         stack_depth=stack_depth, stream=sptr)
+        launch(form, d_out[i], d_head[i:i + 1])
 
     # warm-up (untimed), also the correctness check
     d_out.zero_()
+    d_head.zero_()
     for i in range(args.warmup):
         step(i)
     torch.cuda.synchronize(dev)
@@ -179,6 +194,7 @@ def run_nqb(args):
 
     # timed region: K full counts, pool resident in HBM (630 MB > L2 at n=21 d=7)
     d_out.zero_()
+    d_head.zero_()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if world > 1:
         dist.barrier()
@@ -199,16 +215,34 @@ def run_nqb(args):
     ms_step = ms / args.steps
     value = nodes * world / (ms_step / 1e3)
 
+    # the other form once on the same resident pool, for the plain-vs-batched comparison
+    forms = {args.form: {"ms": round(ms_step, 3), "nodes_per_s": round(nodes / (ms_step / 1e3), 1)}}
+    if not args.skip_other_form:
+        other = "plain" if args.form == "batched" else "batched"
+        o_out = torch.zeros(4, dtype=torch.int64, device=f"cuda:{dev}")
+        o_head = torch.zeros(1, dtype=torch.int32, device=f"cuda:{dev}")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        launch({"plain": nqb.FORM_PLAIN, "batched": nqb.FORM_BATCHED}[other], o_out, o_head)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        o = o_out.cpu().numpy().astype(np.uint64)
+        assert int(o[0]) == count and int(o[1]) == nodes and int(o[3]) == 0
+        oms = e0.elapsed_time(e1)
+        forms[other] = {"ms": round(oms, 3), "nodes_per_s": round(nodes / (oms / 1e3), 1), "steps": 1}
+        if "plain" in forms and "batched" in forms:
+            forms["batched_over_plain"] = round(forms["plain"]["ms"] / forms["batched"]["ms"], 3)
+
     # e2e: the public C ABI call with host buffers, every step
     e2e = None
     if not args.skip_e2e:
-        nqb.count_ex(n, d, device=dev)  # warm-up of the call path
+        nqb.count_ex(n, d, device=dev, form=form)  # warm-up of the call path
         if world > 1:
             dist.barrier()
         walls, gen, h2d, ker = [], [], [], []
         for _ in range(args.steps):
             t0 = time.perf_counter()
-            c, st = nqb.count_ex(n, d, device=dev)
+            c, st = nqb.count_ex(n, d, device=dev, form=form)
             walls.append(time.perf_counter() - t0)
             assert c == count
             gen.append(st["gen_ms"]), h2d.append(st["h2d_ms"]), ker.append(st["kernel_ms"])
@@ -243,13 +277,14 @@ def run_nqb(args):
             "metric": METRIC, "value": round(value, 1), "unit": "nodes/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic (the full depth-7 pool of the N=21 board)",
-            "config": {"workload": f"full count N={n}, pregen depth {d}", "n": n, "depth": d, "form": "plain",
+            "config": {"workload": f"full count N={n}, pregen depth {d}", "n": n, "depth": d, "form": args.form,
                        "states": states, "nodes": nodes, "count": count, "block": args.block or 128,
                        "parallelism": f"replicas{world}" if world > 1 else "single",
                        "l2": f"inputs larger than L2 (pool {states * 16 / 1e6:.0f} MB)"},
+            "forms": forms,
             "e2e": e2e,
             "roofline": roofline(nodes, ms_step / 1e3, sms, max_mhz,
-                                 profile_traffic("plain_search_kernel", n, d)),
+                                 profile_traffic(f"{args.form}_search_kernel", n, d)),
             "cpu_baseline": cpu,
             "clocks": ck,
             "gpu_launches": args.steps * (1 + (states - 1) // (1 << 30)),
@@ -284,8 +319,9 @@ def run_reference(args):
             "cpu_baseline": {"value": round(value, 1), "unit": "nodes/s", "cores": cores, "kind": kind,
                              "sample": sample},
             "e2e": {"value": round(value, 1), "unit": "nodes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    if args.ref_cuda and nqo.ref_available(n):
-        line["reference_cuda"] = reference_cuda(nqo, n, d)
+    rn, rd = args.ref_cuda_n, args.ref_cuda_d
+    if args.ref_cuda and nqo.ref_available(rn):
+        line["reference_cuda"] = reference_cuda(nqo, rn, rd)
     print(json.dumps(line), flush=True)
 
 
@@ -300,9 +336,12 @@ def reference_cuda(nqo, n, d):
     js = [json.loads(l[9:]) for l in p.stdout.splitlines() if l.startswith("NQO_JSON ")]
     km = [float(x) for x in re.findall(r"Time taken: ([0-9.]+)ms", p.stdout)]
     r = js[-1] if js else {}
-    out = {"count": r.get("count"), "count_ok": r.get("count") == KAT.get(n), "kernel_ms": km[-1] if km else None,
+    out = {"workload": f"full count N={n}, pregen depth {d}", "count": r.get("count"),
+           "count_ok": r.get("count") == KAT.get(n), "kernel_ms": km[-1] if km else None,
            "driver_ms": round(1e3 * r.get("driver_seconds", 0), 3), "gen_ms": round(1e3 * r.get("gen_seconds", 0), 3),
            "process_wall_s": round(wall, 3)}
+    if (n, d) in NODES and out["kernel_ms"]:
+        out["nodes_per_s"] = round(NODES[(n, d)] / (out["kernel_ms"] / 1e3), 1)
     return out
 
 
@@ -315,9 +354,13 @@ def main():
     ap.add_argument("--n", type=int, default=21)
     ap.add_argument("--depth", type=int, default=7)
     ap.add_argument("--block", type=int, default=0)
+    ap.add_argument("--form", default="batched", choices=["batched", "plain"])
+    ap.add_argument("--skip-other-form", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-step-seconds", type=float, default=8.0)
     ap.add_argument("--ref-cuda", type=int, default=1)
+    ap.add_argument("--ref-cuda-n", type=int, default=19)
+    ap.add_argument("--ref-cuda-d", type=int, default=7)
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     args = ap.parse_args()

@@ -11,7 +11,7 @@
 //     pending row (the largest piece of its remaining subtree) to an idle lane of the
 //     same warp, which searches it as a new piece of the same item.  Nothing is waited
 //     on: no spin, barrier or flag crosses warps.
-// The search step is search_step.cuh.  A lane's stack holds a zero sentinel at
+// The search step is search_step.cuh.  A lane's stack holds the sentinel entry at
 // `base` and its pending rows above it; giving away the bottom row turns that row's
 // slot into the new sentinel, so base moves up one slot.  Because pending rows are
 // strictly deeper towards the top, sentinel and rows never pass base0 + f - 1 slots

@@ -56,28 +56,25 @@ __global__ void __launch_bounds__(BLOCK) plain_search_kernel(const uint4* __rest
     unsigned long long sols = 0, nodes = 0;
     uint32_t unit = 0;
     bool first = true;
-    for (;;) {
-        bool done = false;
-        for (uint32_t v = 0; v < kEpoch; ++v) {
-            if (__all_sync(kFull, s.avail == 0 && s.sp == base)) {
-                done = true;
-                break;
-            }
-#pragma unroll
-            for (int u = 0; u < kUnroll; ++u) {
-                if (UNIT) {
-                    unit += (!first && s.avail != 0 && (s.avail & (s.avail - 1u)) == 0);
-                    first = false;
-                }
-                search_step<kStride>(s, base);
-            }
+    uint32_t epoch = kEpoch;
+    while (!__all_sync(kFull, s.avail == 0 && s.sp == base)) {
+        if (--epoch == 0) {  // fold lane counters before they can wrap
+            sols += s.sols;
+            nodes += s.nodes;
+            s.sols = s.nodes = 0;
+            epoch = kEpoch;
         }
-        sols += s.sols;
-        nodes += s.nodes;
-        s.sols = 0;
-        s.nodes = 0;
-        if (done) break;
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            if (UNIT) {
+                unit += (!first && s.avail != 0 && (s.avail & (s.avail - 1u)) == 0);
+                first = false;
+            }
+            search_step<kStride>(s, base);
+        }
     }
+    sols += s.sols;
+    nodes += s.nodes;
 
     unsigned long long c = sols * weight;
     if (per_state && gi < count) per_state[gi] = c;
