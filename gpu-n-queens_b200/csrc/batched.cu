@@ -21,6 +21,7 @@
 // totals.  When a lane finishes its piece of an item, the piece's weighted count and
 // nodes go to the warp's totals and, optionally, to per-board slots (64-bit atomics).
 #include <algorithm>
+#include <mutex>
 
 #include "nqb_internal.h"
 #include "search_step.cuh"
@@ -217,3 +218,53 @@ int launch_batched(const nqb_state* d_items, uint32_t n_items, const uint32_t* d
 }
 
 }  // namespace nqb
+
+// ---- Batched launch that allocates nothing -------------------------------------
+//
+// Scratch of nqb_batched_launch_static: the batched kernel's queue head lives in this
+// file-scope device array instead of a buffer the caller allocates.  Every GPU that
+// loads the library holds these 256 bytes until the process exits; word 0 is the queue
+// head, the rest is unused headroom.  In host code `g_static_scratch` only names the
+// symbol: its device address is looked up with cudaGetSymbolAddress, once per device,
+// and that address is what the kernel receives.
+static __device__ __align__(256) uint32_t g_static_scratch[NQB_STATIC_SCRATCH_BYTES / 4];
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mu;
+uint32_t* g_static_addr[kMaxDevices] = {};
+
+// Device address of g_static_scratch on the current device (set up on first use).
+int static_scratch_address(int dev, uint32_t** out) {
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess) return nqb::cuda_status(e);
+        g_static_addr[dev] = static_cast<uint32_t*>(p);
+    }
+    *out = g_static_addr[dev];
+    return NQB_OK;
+}
+
+}  // namespace
+
+extern "C" int nqb_batched_launch_static(const nqb_state* d_items, uint64_t count, const uint32_t* d_order,
+                                         uint64_t* d_out, int block_size, unsigned stack_depth, void* stream) {
+    if (count > NQB_STATIC_MAX_ITEMS) return NQB_E_RANGE;
+    if (!d_out || (count && !d_items)) return NQB_E_INVALID;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return NQB_E_NODEVICE;
+    if (dev < 0 || dev >= kMaxDevices) return NQB_E_RANGE;
+    uint32_t* head = nullptr;
+    const int s = static_scratch_address(dev, &head);
+    if (s != NQB_OK) return s;
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // The array keeps the previous call's head; the queue must start empty.
+    const cudaError_t e = cudaMemsetAsync(head, 0, sizeof(uint32_t), st);
+    if (e != cudaSuccess) return nqb::cuda_status(e);
+    return nqb::launch_batched(d_items, (uint32_t)count, d_order, nullptr, head,
+                               reinterpret_cast<unsigned long long*>(d_out), nullptr, nullptr, block_size,
+                               stack_depth, dev, st, nullptr);
+}

@@ -217,6 +217,36 @@ int nqb_plain_launch(const nqb_state* d_states, uint64_t count, uint64_t* d_out,
 int nqb_batched_launch(const nqb_state* d_items, uint64_t count, const uint32_t* d_order, uint32_t* d_head,
                        uint64_t* d_out, int block_size, unsigned stack_depth, void* stream);
 
+/* Scratch held by nqb_batched_launch_static on every GPU that loads the library. */
+#define NQB_STATIC_SCRATCH_BYTES 256
+/* Largest item count nqb_batched_launch_static accepts (its 32-bit queue head). */
+#define NQB_STATIC_MAX_ITEMS (1ull << 31)
+
+/*
+ * nqb_batched_launch for callers that cannot allocate device memory.  It has no
+ * counterpart in the reference.
+ *
+ * Some callers may not call cudaMalloc or cudaFree at all: code running inside a
+ * stream capture (allocation is not a capturable operation), code whose framework
+ * hands out all device memory through its own caching allocator, and code that must
+ * not stall the GPU (cudaFree synchronises the device).  This entry point needs no
+ * scratch buffer from them: the queue head lives in a 256-byte array of this library's
+ * device memory (NQB_STATIC_SCRATCH_BYTES), which every GPU that loads the library
+ * holds until the process exits.  The caller still passes the items, the optional
+ * order and the four result words, exactly as for nqb_batched_launch; this call
+ * allocates nothing and calls no allocating library routine.
+ *
+ * - The first call on a device looks the array's device address up
+ *   (cudaGetSymbolAddress) with that device current; make that first call before any
+ *   stream capture on the device.
+ * - Each call clears the queue head on `stream` before launching (the array keeps
+ *   whatever the previous call left).  All calls on a device share the one array, so
+ *   calls whose work overlaps on the GPU race: serialise them, e.g. on one stream.
+ * - count > NQB_STATIC_MAX_ITEMS returns NQB_E_RANGE without launching.
+ */
+int nqb_batched_launch_static(const nqb_state* d_items, uint64_t count, const uint32_t* d_order,
+                              uint64_t* d_out, int block_size, unsigned stack_depth, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
