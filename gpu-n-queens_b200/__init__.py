@@ -35,15 +35,16 @@ class NQBError(RuntimeError):
 
 class Opts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("form", ctypes.c_int), ("block_size", ctypes.c_int),
-                ("count_unit_nodes", ctypes.c_int), ("use_model", ctypes.c_int),
-                ("split_depth", ctypes.c_int), ("reserved", ctypes.c_int * 10)]
+                ("count_unit_nodes", ctypes.c_int), ("max_split_rounds", ctypes.c_int),
+                ("split_factor", ctypes.c_int), ("model", ctypes.c_void_p), ("reserved", ctypes.c_int * 8)]
 
 
 class Stats(ctypes.Structure):
     _fields_ = [("states", ctypes.c_uint64), ("nodes", ctypes.c_uint64), ("unit_nodes", ctypes.c_uint64),
                 ("gen_ms", ctypes.c_double), ("h2d_ms", ctypes.c_double), ("kernel_ms", ctypes.c_double),
                 ("wall_ms", ctypes.c_double), ("pregen_depth", ctypes.c_uint32),
-                ("kernel_launches", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 6)]
+                ("kernel_launches", ctypes.c_uint32), ("items", ctypes.c_uint64), ("sched_ms", ctypes.c_double),
+                ("reserved", ctypes.c_uint32 * 2)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
@@ -116,12 +117,13 @@ def _check(status, what):
         raise NQBError(status, what)
 
 
-def make_opts(device=0, form=FORM_PLAIN, block_size=0, count_unit_nodes=False, use_model=False,
-              split_depth=-1):
+def make_opts(device=0, form=FORM_PLAIN, block_size=0, count_unit_nodes=False, model=None, max_split_rounds=-1,
+              split_factor=0):
     o = Opts()
     lib().nqb_default_opts(ctypes.byref(o))
     o.device, o.form, o.block_size = device, form, block_size
-    o.count_unit_nodes, o.use_model, o.split_depth = int(count_unit_nodes), int(use_model), split_depth
+    o.count_unit_nodes, o.max_split_rounds, o.split_factor = int(count_unit_nodes), max_split_rounds, split_factor
+    o.model = model.handle if model is not None else None
     return o
 
 
@@ -248,6 +250,110 @@ def batched_launch(d_items_ptr, count, d_head_ptr, d_out_ptr, d_order_ptr=None, 
     """Launches the batched (persistent, work-queue) kernel on device pointers."""
     _check(lib().nqb_batched_launch(d_items_ptr, count, d_order_ptr, d_head_ptr, d_out_ptr, block_size,
                                     stack_depth, stream or None), "nqb_batched_launch")
+
+
+MODEL_INPUTS, MODEL_PARAMS = 112, 31105
+
+
+class TrainOpts(ctypes.Structure):
+    _fields_ = [("epochs", ctypes.c_int), ("batch", ctypes.c_int), ("lr", ctypes.c_float),
+                ("reserved0", ctypes.c_int), ("seed", ctypes.c_uint64), ("reserved", ctypes.c_int * 8)]
+
+
+def _model_sigs(L):
+    vp, fp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)
+    sig = {
+        "nqb_model_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(vp)]),
+        "nqb_model_destroy": (None, [vp]),
+        "nqb_model_get_params": (ctypes.c_int, [vp, vp]),
+        "nqb_model_set_params": (ctypes.c_int, [vp, vp]),
+        "nqb_model_features": (ctypes.c_int, [vp, ctypes.c_uint64, vp]),
+        "nqb_model_predict": (ctypes.c_int, [vp, vp, ctypes.c_uint64, vp]),
+        "nqb_model_loss_grad": (ctypes.c_int, [vp, vp, vp, ctypes.c_uint64, fp, vp]),
+        "nqb_model_train": (ctypes.c_int, [vp, vp, vp, ctypes.c_uint64, ctypes.POINTER(TrainOpts), vp]),
+        "nqb_record_nodes": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.POINTER(Opts), vp, vp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype, f.argtypes = res, args
+
+
+class Model:
+    """The learned cost model (nqb_model_*): predicts log2(1 + nodes) below a state."""
+
+    def __init__(self, device=0, seed=1):
+        L = lib()
+        _model_sigs(L)
+        h = ctypes.c_void_p()
+        _check(L.nqb_model_create(device, seed, ctypes.byref(h)), "nqb_model_create")
+        self.handle, self.device = h.value, device
+
+    def close(self):
+        if self.handle:
+            lib().nqb_model_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def get_params(self):
+        p = np.zeros(MODEL_PARAMS, dtype=np.float32)
+        _check(lib().nqb_model_get_params(self.handle, p.ctypes.data), "nqb_model_get_params")
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == MODEL_PARAMS
+        _check(lib().nqb_model_set_params(self.handle, p.ctypes.data), "nqb_model_set_params")
+
+    def predict(self, states):
+        states = np.ascontiguousarray(states, dtype=STATE_DTYPE)
+        out = np.zeros(max(len(states), 1), dtype=np.float32)
+        _check(lib().nqb_model_predict(self.handle, states.ctypes.data, len(states), out.ctypes.data),
+               "nqb_model_predict")
+        return out[:len(states)]
+
+    def loss_grad(self, states, targets):
+        states = np.ascontiguousarray(states, dtype=STATE_DTYPE)
+        t = np.ascontiguousarray(targets, dtype=np.float32)
+        g = np.zeros(MODEL_PARAMS, dtype=np.float32)
+        loss = ctypes.c_float(0)
+        _check(lib().nqb_model_loss_grad(self.handle, states.ctypes.data, t.ctypes.data, len(states),
+                                         ctypes.byref(loss), g.ctypes.data), "nqb_model_loss_grad")
+        return loss.value, g
+
+    def train(self, states, targets, epochs=8, batch=4096, lr=1e-3, seed=1):
+        states = np.ascontiguousarray(states, dtype=STATE_DTYPE)
+        t = np.ascontiguousarray(targets, dtype=np.float32)
+        o = TrainOpts(epochs=epochs, batch=batch, lr=lr, seed=seed)
+        losses = np.zeros(epochs, dtype=np.float32)
+        _check(lib().nqb_model_train(self.handle, states.ctypes.data, t.ctypes.data, len(states), ctypes.byref(o),
+                                     losses.ctypes.data), "nqb_model_train")
+        return losses
+
+
+def model_features(states):
+    L = lib()
+    _model_sigs(L)
+    states = np.ascontiguousarray(states, dtype=STATE_DTYPE)
+    out = np.zeros((max(len(states), 1), MODEL_INPUTS), dtype=np.float32)
+    _check(L.nqb_model_features(states.ctypes.data, len(states), out.ctypes.data), "nqb_model_features")
+    return out[:len(states)]
+
+
+def record_nodes(states, device=0):
+    """(nodes, weighted counts) per state, recorded by the batched search kernel."""
+    L = lib()
+    _model_sigs(L)
+    states = np.ascontiguousarray(states, dtype=STATE_DTYPE)
+    nodes = np.zeros(max(len(states), 1), dtype=np.uint64)
+    counts = np.zeros(max(len(states), 1), dtype=np.uint64)
+    _check(L.nqb_record_nodes(states.ctypes.data, len(states), ctypes.byref(make_opts(device=device)),
+                              nodes.ctypes.data, counts.ctypes.data), "nqb_record_nodes")
+    return nodes[:len(states)], counts[:len(states)]
 
 
 def header_symbols():

@@ -91,7 +91,8 @@ bool state_ok(const nqb_state& s) {
 // Solves `count` host states on the device with the form o.form; fills totals
 // {count, nodes, unit, err} and, if per_state != nullptr, per-state weighted counts.
 int solve_host_states(Scope& sc, const nqb_state* states, uint64_t count, const nqb_opts& o,
-                      unsigned long long totals[4], uint64_t* per_state, nqb_stats* st) {
+                      unsigned long long totals[4], uint64_t* per_state, nqb_stats* st,
+                      uint64_t* per_state_nodes = nullptr) {
     for (uint64_t i = 0; i < count; ++i)
         if (!state_ok(states[i])) return NQB_E_INVALID;
     const bool batched = o.form == NQB_FORM_BATCHED;
@@ -104,6 +105,12 @@ int solve_host_states(Scope& sc, const nqb_state* states, uint64_t count, const 
     NQB_TRY(sc.alloc(&d_states, count * sizeof(nqb_state)));
     NQB_TRY(sc.alloc(&d_out, 5 * sizeof(unsigned long long)));
     if (per_state) NQB_TRY(sc.alloc(&d_per, count * sizeof(unsigned long long)));
+    unsigned long long* d_per_nodes = nullptr;
+    if (per_state_nodes) {
+        if (!batched) return NQB_E_INVALID;
+        NQB_TRY(sc.alloc(&d_per_nodes, count * sizeof(unsigned long long)));
+        NQB_TRY(cuda_status(cudaMemsetAsync(d_per_nodes, 0, count * sizeof(unsigned long long), sc.stream)));
+    }
     uint32_t* d_head = reinterpret_cast<uint32_t*>(d_out + 4);
     cudaEvent_t e0, e1, e2;
     NQB_TRY(sc.event(&e0));
@@ -116,9 +123,11 @@ int solve_host_states(Scope& sc, const nqb_state* states, uint64_t count, const 
     if (d_per) NQB_TRY(cuda_status(cudaMemsetAsync(d_per, 0, count * sizeof(unsigned long long), sc.stream)));
     NQB_TRY(cuda_status(cudaEventRecord(e1, sc.stream)));
     unsigned launches = 0;
+    SchedInfo sched;
+    sched.items = count;
     if (batched) {
-        NQB_TRY(launch_batched(d_states, (uint32_t)count, nullptr, nullptr, d_head, d_out, d_per, nullptr,
-                               o.block_size, depth, sc.device, sc.stream, &launches));
+        NQB_TRY(launch_batched_scheduled(d_states, (uint32_t)count, nullptr, d_head, d_out, d_per, d_per_nodes, o,
+                                         depth, sc.device, sc.stream, &launches, &sched));
     } else {
         NQB_TRY(launch_plain(d_states, count, d_out, d_per, o.block_size, o.count_unit_nodes != 0, depth,
                              sc.stream, &launches));
@@ -128,6 +137,9 @@ int solve_host_states(Scope& sc, const nqb_state* states, uint64_t count, const 
                                         sc.stream)));
     if (per_state)
         NQB_TRY(cuda_status(cudaMemcpyAsync(per_state, d_per, count * sizeof(unsigned long long),
+                                            cudaMemcpyDeviceToHost, sc.stream)));
+    if (per_state_nodes)
+        NQB_TRY(cuda_status(cudaMemcpyAsync(per_state_nodes, d_per_nodes, count * sizeof(unsigned long long),
                                             cudaMemcpyDeviceToHost, sc.stream)));
     NQB_TRY(cuda_status(cudaStreamSynchronize(sc.stream)));
     if (totals[3]) return NQB_E_DEVICE;
@@ -141,6 +153,8 @@ int solve_host_states(Scope& sc, const nqb_state* states, uint64_t count, const 
         st->h2d_ms = h2d;
         st->kernel_ms = ker;
         st->kernel_launches = launches;
+        st->items = sched.items;
+        st->sched_ms = sched.sched_ms;
     }
     return NQB_OK;
 }
@@ -164,7 +178,9 @@ void nqb_default_opts(nqb_opts* o) {
     o->device = 0;
     o->form = NQB_FORM_PLAIN;
     o->block_size = 0;
-    o->split_depth = -1;
+    o->max_split_rounds = -1;
+    o->split_factor = 0;
+    o->model = nullptr;
 }
 
 const char* nqb_strerror(int s) {
@@ -283,6 +299,19 @@ int nqb_solve_batch(const nqb_state* boards, uint64_t count, const nqb_opts* opt
     NQB_TRY(solve_host_states(sc, boards, count, o, totals, out, stats));
     if (stats) stats->wall_ms = now_ms() - t0;
     return NQB_OK;
+}
+
+int nqb_record_nodes(const nqb_state* states, uint64_t count, const nqb_opts* opts, uint64_t* nodes,
+                     uint64_t* counts) {
+    if (!nodes || !counts || (count && !states)) return NQB_E_INVALID;
+    if (count == 0) return NQB_OK;
+    nqb_opts o = resolve(opts);
+    o.form = NQB_FORM_BATCHED;
+    o.model = nullptr;
+    Scope sc(o.device);
+    NQB_TRY(sc.status);
+    unsigned long long totals[4] = {0, 0, 0, 0};
+    return solve_host_states(sc, states, count, o, totals, counts, nullptr, nodes);
 }
 
 size_t nqb_ref_state_size(unsigned n) {

@@ -31,8 +31,11 @@ namespace {
 
 constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr uint32_t kNoItem = 0xFFFFFFFFu;
-constexpr int kUnroll = 8;
-constexpr uint32_t kEpoch = 1u << 26;  // rounds between folds: kUnroll x kEpoch < 2^32
+#ifndef NQB_BATCHED_UNROLL
+#define NQB_BATCHED_UNROLL 16
+#endif
+constexpr int kUnroll = NQB_BATCHED_UNROLL;  // search steps between idle-lane checks
+constexpr uint32_t kEpoch = 1u << 26;        // rounds between folds: kUnroll x kEpoch < 2^32
 
 struct BatchArgs {
     const uint4* items;        // search states (nqb_state layout)

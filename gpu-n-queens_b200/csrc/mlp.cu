@@ -1,0 +1,674 @@
+// Learned cost model: an MLP 112 -> 128 -> 128 -> 1 (GELU) that predicts log2 of the number
+// of search nodes below a state.  Trained on the GPU by the kernels in this file (FP16
+// operands, FP32 accumulation on the tensor cores through mma.sync m16n8k16; FP32 master
+// weights, Adam), on node counts the batched search kernel records per item.  Used only to
+// order and split the batched form's queue (schedule.cu); counts never depend on it.
+//
+// Training step on a batch of B rows (X: B x 112 fp16):
+//   Z1 = X W1           H1 = gelu(Z1 + b1)      (fp16 copy of H1 feeds the next GEMM)
+//   Z2 = H1 W2          H2 = gelu(Z2 + b2)
+//   y  = H2 w3 + b3     loss = mean (y - t)^2
+//   dy = 2 (y - t)      dZ2 = dy w3^T * gelu'(Z2 + b2)      dH1 = dZ2 W2^T
+//   dZ1 = dH1 * gelu'(Z1 + b1)
+//   dW2 = H1^T dZ2 / B  dW1 = X^T dZ1 / B  dw3 = H2^T dy / B  (bias grads: column sums / B)
+// All GEMMs go through one tiled kernel with arbitrary operand strides (gemm_f16).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <type_traits>
+#include <vector>
+
+#include "mlp.cuh"
+#include "nqb_internal.h"
+
+namespace nqb {
+namespace mlp {
+namespace {
+
+// ---- generic GEMM: C (M x N, fp32, row-major ldc) = alpha * A x B + beta * C -----------
+// A(i, k) = A[i * sai + k * sak], B(k, j) = B[k * sbk + j * sbj], fp16.  Block tile 64 x 64,
+// 4 warps, each 16 rows x 64 columns (8 MMA n-tiles); K in steps of 16.
+constexpr int kTile = 64;
+constexpr int kKs = 16;
+constexpr int kPad = 8;  // row padding (halves) that keeps fragment loads conflict-free
+
+__global__ void __launch_bounds__(128) gemm_f16(const __half* __restrict__ A, long sai, long sak,
+                                                const __half* __restrict__ B, long sbk, long sbj,
+                                                float* __restrict__ C, long ldc, int M, int N, int K, float alpha,
+                                                float beta) {
+    __shared__ __align__(16) __half As[kTile][kKs + kPad];
+    __shared__ __align__(16) __half Bs[kTile][kKs + kPad];  // [n][k]
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int bm = blockIdx.y * kTile, bn = blockIdx.x * kTile;
+    float acc[8][4];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.0f;
+    for (int k0 = 0; k0 < K; k0 += kKs) {
+        for (int e = tid; e < kTile * kKs; e += 128) {
+            const int r = e / kKs, kk = e % kKs;
+            const int gi = bm + r, gj = bn + r, gk = k0 + kk;
+            As[r][kk] = (gi < M && gk < K) ? A[gi * sai + gk * sak] : __float2half(0.0f);
+            Bs[r][kk] = (gj < N && gk < K) ? B[gk * sbk + gj * sbj] : __float2half(0.0f);
+        }
+        __syncthreads();
+        const int r0 = warp * 16 + g;
+        const uint32_t a0 = *reinterpret_cast<const uint32_t*>(&As[r0][2 * t]);
+        const uint32_t a1 = *reinterpret_cast<const uint32_t*>(&As[r0 + 8][2 * t]);
+        const uint32_t a2 = *reinterpret_cast<const uint32_t*>(&As[r0][2 * t + 8]);
+        const uint32_t a3 = *reinterpret_cast<const uint32_t*>(&As[r0 + 8][2 * t + 8]);
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) {
+            const uint32_t b0 = *reinterpret_cast<const uint32_t*>(&Bs[nt * 8 + g][2 * t]);
+            const uint32_t b1 = *reinterpret_cast<const uint32_t*>(&Bs[nt * 8 + g][2 * t + 8]);
+            mma16816(acc[nt], a0, a1, a2, a3, b0, b1);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int i = bm + warp * 16 + g + 8 * h;
+            if (i >= M) continue;
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const int j = bn + nt * 8 + 2 * t + c;
+                if (j >= N) continue;
+                float* p = C + (long)i * ldc + j;
+                const float v = alpha * acc[nt][2 * h + c];
+                *p = beta == 0.0f ? v : v + beta * *p;
+            }
+        }
+    }
+}
+
+int gemm(const __half* A, long sai, long sak, const __half* B, long sbk, long sbj, float* C, long ldc, int M, int N,
+         int K, float alpha, float beta, cudaStream_t s) {
+    if (M <= 0 || N <= 0 || K <= 0) return NQB_OK;
+    const dim3 grid((N + kTile - 1) / kTile, (M + kTile - 1) / kTile);
+    gemm_f16<<<grid, 128, 0, s>>>(A, sai, sak, B, sbk, sbj, C, ldc, M, N, K, alpha, beta);
+    return cuda_status(cudaGetLastError());
+}
+
+// ---- elementwise and reduction kernels -------------------------------------------------
+__global__ void features_kernel(const uint4* __restrict__ st, const uint32_t* __restrict__ rows, uint32_t n_rows,
+                                __half* __restrict__ X) {
+    const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (uint64_t)n_rows * kIn) return;
+    const uint32_t i = (uint32_t)(e / kIn), j = (uint32_t)(e % kIn);
+    const uint4 s = st[rows ? rows[i] : i];
+    X[e] = __float2half(feature(s, (int)j));
+}
+
+// H = gelu(Z + b) (fp16), Zb = Z + b kept for the backward pass.
+__global__ void bias_gelu_kernel(const float* __restrict__ Z, const float* __restrict__ b, uint32_t rows,
+                                 float* __restrict__ Zb, __half* __restrict__ H) {
+    const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (uint64_t)rows * kH) return;
+    const float z = Z[e] + b[e % kH];
+    Zb[e] = z;
+    H[e] = __float2half(gelu(z));
+}
+
+// y_i = H2_i . w3 + b3 (one warp per row).
+__global__ void head_kernel(const __half* __restrict__ H2, const float* __restrict__ w3, const float* __restrict__ b3,
+                            uint32_t rows, float* __restrict__ y) {
+    const uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (row >= rows) return;
+    float s = 0.0f;
+    for (int j = lane; j < kH; j += 32) s += __half2float(H2[(uint64_t)row * kH + j]) * w3[j];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
+    if (lane == 0) y[row] = s + b3[0];
+}
+
+// dy = 2 (y - t); the squared error is summed into loss[0].
+__global__ void loss_kernel(const float* __restrict__ y, const float* __restrict__ t, uint32_t rows,
+                            float* __restrict__ dy, float* __restrict__ loss) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    float e2 = 0.0f;
+    if (i < rows) {
+        const float d = y[i] - t[i];
+        dy[i] = 2.0f * d;
+        e2 = d * d;
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) e2 += __shfl_xor_sync(0xFFFFFFFFu, e2, o);
+    if ((threadIdx.x & 31) == 0 && e2 != 0.0f) atomicAdd(loss, e2);
+}
+
+// dZ2 = dy_i * w3_j * gelu'(Zb2_ij), fp16.
+__global__ void dz2_kernel(const float* __restrict__ dy, const float* __restrict__ w3, const float* __restrict__ Zb2,
+                           uint32_t rows, __half* __restrict__ dZ2) {
+    const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (uint64_t)rows * kH) return;
+    dZ2[e] = __float2half(dy[e / kH] * w3[e % kH] * gelu_grad(Zb2[e]));
+}
+
+// dZ1 = dH1 * gelu'(Zb1), fp16.
+__global__ void dz1_kernel(const float* __restrict__ dH1, const float* __restrict__ Zb1, uint32_t rows,
+                           __half* __restrict__ dZ1) {
+    const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (uint64_t)rows * kH) return;
+    dZ1[e] = __float2half(dH1[e] * gelu_grad(Zb1[e]));
+}
+
+// out[j] = scale * sum_i D[i][j] (D fp16 rows x 128); with dy != null: scale * sum_i dy_i D[i][j].
+__global__ void colsum_kernel(const __half* __restrict__ D, const float* __restrict__ dy, uint32_t rows, float scale,
+                              float* __restrict__ out) {
+    const int j = threadIdx.x;  // blockDim = 128
+    float s = 0.0f;
+    for (uint32_t i = blockIdx.x; i < rows; i += gridDim.x) {
+        const float v = __half2float(D[(uint64_t)i * kH + j]);
+        s += dy ? v * dy[i] : v;
+    }
+    atomicAdd(out + j, s * scale);
+}
+
+__global__ void sum_kernel(const float* __restrict__ v, uint32_t n, float scale, float* __restrict__ out) {
+    float s = 0.0f;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += v[i];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, s * scale);
+}
+
+__global__ void gather_f16_rows(const __half* __restrict__ X, const uint32_t* __restrict__ rows, uint32_t n_rows,
+                                __half* __restrict__ out) {
+    const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (uint64_t)n_rows * kIn) return;
+    out[e] = X[(uint64_t)rows[e / kIn] * kIn + e % kIn];
+}
+
+__global__ void gather_f32(const float* __restrict__ v, const uint32_t* __restrict__ rows, uint32_t n,
+                           float* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = v[rows[i]];
+}
+
+// Adam (Kingma & Ba 2015) on the flat fp32 parameters; refreshes the fp16 copies of W1, W2.
+__global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ grad, float* __restrict__ m,
+                            float* __restrict__ v, int n, float lr, float b1, float b2, float eps, float c1, float c2,
+                            __half* __restrict__ w1h, __half* __restrict__ w2h) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = grad[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float w = p[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    p[i] = w;
+    if (i < kW1Size) w1h[i] = __float2half(w);
+    else if (i >= kW2 && i < kB2) w2h[i - kW2] = __float2half(w);
+}
+
+__global__ void to_half_kernel(const float* __restrict__ p, __half* __restrict__ w1h, __half* __restrict__ w2h) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < kW1Size) w1h[i] = __float2half(p[kW1 + i]);
+    if (i < kH * kH) w2h[i] = __float2half(p[kW2 + i]);
+}
+
+// ---- fused inference: features -> layer 1 -> layer 2 -> head, 64 states per tile ------
+// Weights stay in shared memory for the whole (persistent) block: W1 and W2 transposed to
+// [out][in] so an MMA B fragment is one 32-bit load.  Each warp owns 16 rows of a tile.
+constexpr int kXs = kIn + 8;  // padded row lengths (halves)
+constexpr int kHs = kH + 8;
+constexpr size_t kPredictSmem = (size_t)(kH * kXs + kH * kHs + 64 * kXs + 64 * kHs) * sizeof(__half) +
+                                (3 * kH + 4) * sizeof(float);
+
+__global__ void __launch_bounds__(128) predict_kernel(const uint4* __restrict__ st, uint32_t count,
+                                                      const __half* __restrict__ w1h, const __half* __restrict__ w2h,
+                                                      const float* __restrict__ params, float* __restrict__ out) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __half* W1s = reinterpret_cast<__half*>(smem);
+    __half* W2s = W1s + kH * kXs;
+    __half* Xs = W2s + kH * kHs;
+    __half* Hs = Xs + 64 * kXs;
+    float* vec = reinterpret_cast<float*>(Hs + 64 * kHs);  // b1 | b2 | w3 | b3
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+    for (int e = tid; e < kIn * kH; e += 128) W1s[(e % kH) * kXs + e / kH] = w1h[e];
+    for (int e = tid; e < kH * kH; e += 128) W2s[(e % kH) * kHs + e / kH] = w2h[e];
+    for (int e = tid; e < kH; e += 128) {
+        vec[e] = params[kB1 + e];
+        vec[kH + e] = params[kB2 + e];
+        vec[2 * kH + e] = params[kW3 + e];
+    }
+    if (tid == 0) vec[3 * kH] = params[kB3];
+    __syncthreads();
+    const int r0 = warp * 16 + g;
+    for (uint32_t tile = blockIdx.x; (uint64_t)tile * 64 < count; tile += gridDim.x) {
+        for (int e = tid; e < 64 * kIn; e += 128) {
+            const int r = e / kIn, j = e % kIn;
+            const uint64_t i = (uint64_t)tile * 64 + r;
+            Xs[r * kXs + j] = __float2half(i < count ? feature(st[i], j) : 0.0f);
+        }
+        __syncthreads();
+        float acc[16][4];
+#pragma unroll
+        for (int nt = 0; nt < 16; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.0f;
+#pragma unroll
+        for (int ks = 0; ks < kIn; ks += 16) {
+            const uint32_t a0 = *reinterpret_cast<const uint32_t*>(&Xs[r0 * kXs + ks + 2 * t]);
+            const uint32_t a1 = *reinterpret_cast<const uint32_t*>(&Xs[(r0 + 8) * kXs + ks + 2 * t]);
+            const uint32_t a2 = *reinterpret_cast<const uint32_t*>(&Xs[r0 * kXs + ks + 2 * t + 8]);
+            const uint32_t a3 = *reinterpret_cast<const uint32_t*>(&Xs[(r0 + 8) * kXs + ks + 2 * t + 8]);
+#pragma unroll
+            for (int nt = 0; nt < 16; ++nt) {
+                const __half* bp = &W1s[(nt * 8 + g) * kXs + ks + 2 * t];
+                mma16816(acc[nt], a0, a1, a2, a3, *reinterpret_cast<const uint32_t*>(bp),
+                         *reinterpret_cast<const uint32_t*>(bp + 8));
+            }
+        }
+#pragma unroll
+        for (int nt = 0; nt < 16; ++nt)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    const int j = nt * 8 + 2 * t + c;
+                    Hs[(r0 + 8 * h) * kHs + j] = __float2half(gelu(acc[nt][2 * h + c] + vec[j]));
+                }
+        __syncwarp();
+#pragma unroll
+        for (int nt = 0; nt < 16; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.0f;
+#pragma unroll
+        for (int ks = 0; ks < kH; ks += 16) {
+            const uint32_t a0 = *reinterpret_cast<const uint32_t*>(&Hs[r0 * kHs + ks + 2 * t]);
+            const uint32_t a1 = *reinterpret_cast<const uint32_t*>(&Hs[(r0 + 8) * kHs + ks + 2 * t]);
+            const uint32_t a2 = *reinterpret_cast<const uint32_t*>(&Hs[r0 * kHs + ks + 2 * t + 8]);
+            const uint32_t a3 = *reinterpret_cast<const uint32_t*>(&Hs[(r0 + 8) * kHs + ks + 2 * t + 8]);
+#pragma unroll
+            for (int nt = 0; nt < 16; ++nt) {
+                const __half* bp = &W2s[(nt * 8 + g) * kHs + ks + 2 * t];
+                mma16816(acc[nt], a0, a1, a2, a3, *reinterpret_cast<const uint32_t*>(bp),
+                         *reinterpret_cast<const uint32_t*>(bp + 8));
+            }
+        }
+        float s0 = 0.0f, s1 = 0.0f;
+#pragma unroll
+        for (int nt = 0; nt < 16; ++nt)
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const int j = nt * 8 + 2 * t + c;
+                // H2 rounded to fp16 as in the training forward pass (head_kernel reads fp16 H2)
+                s0 += __half2float(__float2half(gelu(acc[nt][c] + vec[kH + j]))) * vec[2 * kH + j];
+                s1 += __half2float(__float2half(gelu(acc[nt][2 + c] + vec[kH + j]))) * vec[2 * kH + j];
+            }
+        s0 += __shfl_xor_sync(0xFFFFFFFFu, s0, 1);
+        s0 += __shfl_xor_sync(0xFFFFFFFFu, s0, 2);
+        s1 += __shfl_xor_sync(0xFFFFFFFFu, s1, 1);
+        s1 += __shfl_xor_sync(0xFFFFFFFFu, s1, 2);
+        if (t == 0) {
+            const uint64_t i = (uint64_t)tile * 64 + r0;
+            if (i < count) out[i] = s0 + vec[3 * kH];
+            if (i + 8 < count) out[i + 8] = s1 + vec[3 * kH];
+        }
+        __syncthreads();
+    }
+}
+
+// Device buffers of one training or gradient pass over batches of up to `cap` rows.
+struct Work {
+    __half *X = nullptr, *H1 = nullptr, *H2 = nullptr, *dZ2 = nullptr, *dZ1 = nullptr;
+    float *t = nullptr, *Z = nullptr, *Zb1 = nullptr, *Zb2 = nullptr, *y = nullptr, *dy = nullptr, *dH1 = nullptr,
+          *loss = nullptr;
+    uint32_t cap = 0;
+    std::vector<void*> owned;
+
+    int init(uint32_t rows) {
+        cap = rows;
+        const size_t r = rows;
+        auto get = [&](auto** p, size_t bytes) {
+            void* v = nullptr;
+            const int s = cuda_status(cudaMalloc(&v, bytes ? bytes : 16));
+            if (s == NQB_OK) {
+                owned.push_back(v);
+                *p = static_cast<std::remove_pointer_t<decltype(p)>>(v);
+            }
+            return s;
+        };
+        int s = NQB_OK;
+        if (!s) s = get(&X, r * kIn * sizeof(__half));
+        if (!s) s = get(&H1, r * kH * sizeof(__half));
+        if (!s) s = get(&H2, r * kH * sizeof(__half));
+        if (!s) s = get(&dZ2, r * kH * sizeof(__half));
+        if (!s) s = get(&dZ1, r * kH * sizeof(__half));
+        if (!s) s = get(&t, r * sizeof(float));
+        if (!s) s = get(&Z, r * kH * sizeof(float));
+        if (!s) s = get(&Zb1, r * kH * sizeof(float));
+        if (!s) s = get(&Zb2, r * kH * sizeof(float));
+        if (!s) s = get(&y, r * sizeof(float));
+        if (!s) s = get(&dy, r * sizeof(float));
+        if (!s) s = get(&dH1, r * kH * sizeof(float));
+        if (!s) s = get(&loss, sizeof(float));
+        return s;
+    }
+    ~Work() {
+        for (void* p : owned) cudaFree(p);
+    }
+};
+
+unsigned blocks_for(uint64_t n, unsigned per = 256) { return (unsigned)((n + per - 1) / per); }
+
+}  // namespace
+}  // namespace mlp
+}  // namespace nqb
+
+// ---- the model object ---------------------------------------------------------------------
+struct nqb_model {
+    int device = 0;
+    float* params = nullptr;  // fp32 master weights (kParams)
+    float* grad = nullptr;
+    float* m = nullptr;  // Adam moments
+    float* v = nullptr;
+    __half* w1h = nullptr;  // fp16 copies fed to the tensor cores
+    __half* w2h = nullptr;
+    long adam_step = 0;
+};
+
+namespace nqb {
+namespace mlp {
+namespace {
+
+// Forward and backward over `rows` rows already in w.X / w.t; accumulates the mean
+// squared error into w.loss and writes the mean gradient into m->grad.
+int pass(nqb_model* m, Work& w, uint32_t rows, cudaStream_t s) {
+    const float* P = m->params;
+    float* G = m->grad;
+    int st;
+    cudaMemsetAsync(G, 0, kParams * sizeof(float), s);
+    // forward
+    if ((st = gemm(w.X, kIn, 1, m->w1h, kH, 1, w.Z, kH, rows, kH, kIn, 1.0f, 0.0f, s))) return st;
+    bias_gelu_kernel<<<blocks_for((uint64_t)rows * kH), 256, 0, s>>>(w.Z, P + kB1, rows, w.Zb1, w.H1);
+    if ((st = gemm(w.H1, kH, 1, m->w2h, kH, 1, w.Z, kH, rows, kH, kH, 1.0f, 0.0f, s))) return st;
+    bias_gelu_kernel<<<blocks_for((uint64_t)rows * kH), 256, 0, s>>>(w.Z, P + kB2, rows, w.Zb2, w.H2);
+    head_kernel<<<blocks_for((uint64_t)rows * 32), 256, 0, s>>>(w.H2, P + kW3, P + kB3, rows, w.y);
+    loss_kernel<<<blocks_for(rows), 256, 0, s>>>(w.y, w.t, rows, w.dy, w.loss);
+    // backward (mean over the rows)
+    const float inv = 1.0f / (float)rows;
+    colsum_kernel<<<std::min<unsigned>(rows, 512), kH, 0, s>>>(w.H2, w.dy, rows, inv, G + kW3);  // dw3
+    sum_kernel<<<std::min<unsigned>(blocks_for(rows), 256), 256, 0, s>>>(w.dy, rows, inv, G + kB3);
+    dz2_kernel<<<blocks_for((uint64_t)rows * kH), 256, 0, s>>>(w.dy, P + kW3, w.Zb2, rows, w.dZ2);
+    colsum_kernel<<<std::min<unsigned>(rows, 512), kH, 0, s>>>(w.dZ2, nullptr, rows, inv, G + kB2);
+    // dW2 = H1^T dZ2: A(i, k) = H1[k][i], B(k, j) = dZ2[k][j]
+    if ((st = gemm(w.H1, 1, kH, w.dZ2, kH, 1, G + kW2, kH, kH, kH, rows, inv, 0.0f, s))) return st;
+    // dH1 = dZ2 W2^T: B(k, j) = W2[j][k]
+    if ((st = gemm(w.dZ2, kH, 1, m->w2h, 1, kH, w.dH1, kH, rows, kH, kH, 1.0f, 0.0f, s))) return st;
+    dz1_kernel<<<blocks_for((uint64_t)rows * kH), 256, 0, s>>>(w.dH1, w.Zb1, rows, w.dZ1);
+    colsum_kernel<<<std::min<unsigned>(rows, 512), kH, 0, s>>>(w.dZ1, nullptr, rows, inv, G + kB1);
+    // dW1 = X^T dZ1
+    if ((st = gemm(w.X, 1, kIn, w.dZ1, kH, 1, G + kW1, kH, kIn, kH, rows, inv, 0.0f, s))) return st;
+    return cuda_status(cudaGetLastError());
+}
+
+// Seeded uniform initialisation: W ~ U(-sqrt(6/(fan_in+fan_out)), +) (Glorot), biases 0,
+// b3 = the mean target so the first steps start near the data.
+void init_params(std::vector<float>& p, uint64_t seed) {
+    p.assign(kParams, 0.0f);
+    uint64_t st = seed ? seed : 0x9E3779B97F4A7C15ull;
+    auto next = [&]() {
+        uint64_t z = (st += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+    };
+    auto fill = [&](int off, int n, int fin, int fout) {
+        const double a = std::sqrt(6.0 / (fin + fout));
+        for (int i = 0; i < n; ++i) p[off + i] = (float)((2.0 * next() - 1.0) * a);
+    };
+    fill(kW1, kIn * kH, 100, kH);  // 100 live inputs of the 112
+    fill(kW2, kH * kH, kH, kH);
+    fill(kW3, kH, kH, 1);
+}
+
+}  // namespace
+}  // namespace mlp
+}  // namespace nqb
+
+using namespace nqb;
+using namespace nqb::mlp;
+
+namespace {
+
+struct CallScope {  // current device for the call, restored afterwards; one stream
+    int prev = 0;
+    cudaStream_t s = nullptr;
+    int status = NQB_OK;
+    explicit CallScope(int dev) {
+        cudaGetDevice(&prev);
+        if ((status = cuda_status(cudaSetDevice(dev)))) return;
+        status = cuda_status(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    }
+    ~CallScope() {
+        if (s) {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+        cudaSetDevice(prev);
+    }
+};
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    int alloc(size_t n) { return cuda_status(cudaMalloc(&p, (n ? n : 1) * sizeof(T))); }
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+};
+
+int refresh_half(nqb_model* m, cudaStream_t s) {
+    to_half_kernel<<<blocks_for(kH * kH), 256, 0, s>>>(m->params, m->w1h, m->w2h);
+    return cuda_status(cudaGetLastError());
+}
+
+}  // namespace
+
+extern "C" {
+
+int nqb_model_create(int device, uint64_t seed, nqb_model** out) {
+    if (!out) return NQB_E_INVALID;
+    *out = nullptr;
+    int st = nqb_device_check(device);
+    if (st) return st;
+    CallScope cs(device);
+    if (cs.status) return cs.status;
+    nqb_model* m = new nqb_model();
+    m->device = device;
+    std::vector<float> p;
+    init_params(p, seed);
+    st = cuda_status(cudaMalloc(&m->params, kParams * sizeof(float)));
+    if (!st) st = cuda_status(cudaMalloc(&m->grad, kParams * sizeof(float)));
+    if (!st) st = cuda_status(cudaMalloc(&m->m, kParams * sizeof(float)));
+    if (!st) st = cuda_status(cudaMalloc(&m->v, kParams * sizeof(float)));
+    if (!st) st = cuda_status(cudaMalloc(&m->w1h, kW1Size * sizeof(__half)));
+    if (!st) st = cuda_status(cudaMalloc(&m->w2h, kH * kH * sizeof(__half)));
+    if (!st) st = cuda_status(cudaMemcpyAsync(m->params, p.data(), kParams * sizeof(float), cudaMemcpyHostToDevice, cs.s));
+    if (!st) st = cuda_status(cudaMemsetAsync(m->m, 0, kParams * sizeof(float), cs.s));
+    if (!st) st = cuda_status(cudaMemsetAsync(m->v, 0, kParams * sizeof(float), cs.s));
+    if (!st) st = refresh_half(m, cs.s);
+    if (!st) st = cuda_status(cudaStreamSynchronize(cs.s));
+    if (st) {
+        nqb_model_destroy(m);
+        return st;
+    }
+    *out = m;
+    return NQB_OK;
+}
+
+void nqb_model_destroy(nqb_model* m) {
+    if (!m) return;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(m->device);
+    cudaFree(m->params);
+    cudaFree(m->grad);
+    cudaFree(m->m);
+    cudaFree(m->v);
+    cudaFree(m->w1h);
+    cudaFree(m->w2h);
+    cudaSetDevice(prev);
+    delete m;
+}
+
+int nqb_model_get_params(const nqb_model* m, float* out) {
+    if (!m || !out) return NQB_E_INVALID;
+    CallScope cs(m->device);
+    if (cs.status) return cs.status;
+    int st = cuda_status(cudaMemcpyAsync(out, m->params, kParams * sizeof(float), cudaMemcpyDeviceToHost, cs.s));
+    if (!st) st = cuda_status(cudaStreamSynchronize(cs.s));
+    return st;
+}
+
+int nqb_model_set_params(nqb_model* m, const float* in) {
+    if (!m || !in) return NQB_E_INVALID;
+    CallScope cs(m->device);
+    if (cs.status) return cs.status;
+    int st = cuda_status(cudaMemcpyAsync(m->params, in, kParams * sizeof(float), cudaMemcpyHostToDevice, cs.s));
+    if (!st) st = cuda_status(cudaMemsetAsync(m->m, 0, kParams * sizeof(float), cs.s));
+    if (!st) st = cuda_status(cudaMemsetAsync(m->v, 0, kParams * sizeof(float), cs.s));
+    if (!st) st = refresh_half(m, cs.s);
+    if (!st) st = cuda_status(cudaStreamSynchronize(cs.s));
+    m->adam_step = 0;
+    return st;
+}
+
+int nqb_model_features(const nqb_state* states, uint64_t count, float* out) {
+    if (count && (!states || !out)) return NQB_E_INVALID;
+    for (uint64_t i = 0; i < count; ++i) {
+        uint4 st;
+        std::memcpy(&st, &states[i], sizeof(st));
+        for (int j = 0; j < kIn; ++j) out[i * kIn + j] = feature(st, j);
+    }
+    return NQB_OK;
+}
+
+int nqb_model_predict(const nqb_model* m, const nqb_state* states, uint64_t count, float* out) {
+    if (!m || (count && (!states || !out))) return NQB_E_INVALID;
+    if (count == 0) return NQB_OK;
+    if (count > 0xFFFFFFFFull) return NQB_E_RANGE;
+    CallScope cs(m->device);
+    if (cs.status) return cs.status;
+    DevBuf<nqb_state> d_st;
+    DevBuf<float> d_out;
+    int st = d_st.alloc(count);
+    if (!st) st = d_out.alloc(count);
+    if (!st) st = cuda_status(cudaMemcpyAsync(d_st.p, states, count * sizeof(nqb_state), cudaMemcpyHostToDevice, cs.s));
+    if (!st) st = nqb::model_predict_device(m, d_st.p, (uint32_t)count, d_out.p, cs.s);
+    if (!st) st = cuda_status(cudaMemcpyAsync(out, d_out.p, count * sizeof(float), cudaMemcpyDeviceToHost, cs.s));
+    if (!st) st = cuda_status(cudaStreamSynchronize(cs.s));
+    return st;
+}
+
+int nqb_model_loss_grad(nqb_model* m, const nqb_state* states, const float* targets, uint64_t count, float* loss,
+                        float* grad) {
+    if (!m || !states || !targets || !loss || !grad || count == 0) return NQB_E_INVALID;
+    if (count > (1u << 20)) return NQB_E_RANGE;
+    CallScope cs(m->device);
+    if (cs.status) return cs.status;
+    Work w;
+    DevBuf<nqb_state> d_st;
+    int st = w.init((uint32_t)count);
+    if (!st) st = d_st.alloc(count);
+    if (!st) st = cuda_status(cudaMemcpyAsync(d_st.p, states, count * sizeof(nqb_state), cudaMemcpyHostToDevice, cs.s));
+    if (!st) st = cuda_status(cudaMemcpyAsync(w.t, targets, count * sizeof(float), cudaMemcpyHostToDevice, cs.s));
+    if (st) return st;
+    features_kernel<<<blocks_for(count * kIn), 256, 0, cs.s>>>(reinterpret_cast<const uint4*>(d_st.p), nullptr,
+                                                                 (uint32_t)count, w.X);
+    cudaMemsetAsync(w.loss, 0, sizeof(float), cs.s);
+    if ((st = pass(m, w, (uint32_t)count, cs.s))) return st;
+    float l = 0;
+    st = cuda_status(cudaMemcpyAsync(&l, w.loss, sizeof(float), cudaMemcpyDeviceToHost, cs.s));
+    if (!st) st = cuda_status(cudaMemcpyAsync(grad, m->grad, kParams * sizeof(float), cudaMemcpyDeviceToHost, cs.s));
+    if (!st) st = cuda_status(cudaStreamSynchronize(cs.s));
+    *loss = l / (float)count;
+    return st;
+}
+
+int nqb_model_train(nqb_model* m, const nqb_state* states, const float* targets, uint64_t count,
+                    const nqb_train_opts* opts, float* epoch_loss) {
+    if (!m || !states || !targets || count == 0) return NQB_E_INVALID;
+    if (count > 0xFFFFFFFFull) return NQB_E_RANGE;
+    nqb_train_opts o;
+    std::memset(&o, 0, sizeof(o));
+    o.epochs = 8;
+    o.batch = 4096;
+    o.lr = 1e-3f;
+    o.seed = 1;
+    if (opts) o = *opts;
+    if (o.epochs <= 0 || o.batch <= 0 || o.batch > (1 << 20) || !(o.lr > 0.0f)) return NQB_E_INVALID;
+    CallScope cs(m->device);
+    if (cs.status) return cs.status;
+    const uint32_t B = (uint32_t)std::min<uint64_t>(o.batch, count);
+    Work w;
+    DevBuf<nqb_state> d_st;
+    DevBuf<__half> d_X;
+    DevBuf<float> d_t;
+    DevBuf<uint32_t> d_perm;
+    int st = w.init(B);
+    if (!st) st = d_st.alloc(count);
+    if (!st) st = d_X.alloc(count * kIn);
+    if (!st) st = d_t.alloc(count);
+    if (!st) st = d_perm.alloc(count);
+    if (!st) st = cuda_status(cudaMemcpyAsync(d_st.p, states, count * sizeof(nqb_state), cudaMemcpyHostToDevice, cs.s));
+    if (!st) st = cuda_status(cudaMemcpyAsync(d_t.p, targets, count * sizeof(float), cudaMemcpyHostToDevice, cs.s));
+    if (st) return st;
+    features_kernel<<<blocks_for(count * kIn), 256, 0, cs.s>>>(reinterpret_cast<const uint4*>(d_st.p), nullptr,
+                                                                 (uint32_t)count, d_X.p);
+    std::vector<uint32_t> perm(count);
+    for (uint64_t i = 0; i < count; ++i) perm[i] = (uint32_t)i;
+    uint64_t rng = o.seed * 0x9E3779B97F4A7C15ull + 1;
+    auto next = [&]() {
+        uint64_t z = (rng += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    };
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    for (int ep = 0; ep < o.epochs; ++ep) {
+        for (uint64_t i = count - 1; i > 0; --i) std::swap(perm[i], perm[next() % (i + 1)]);  // Fisher-Yates
+        st = cuda_status(cudaMemcpyAsync(d_perm.p, perm.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice, cs.s));
+        if (st) return st;
+        cudaMemsetAsync(w.loss, 0, sizeof(float), cs.s);
+        for (uint64_t off = 0; off < count; off += B) {
+            const uint32_t rows = (uint32_t)std::min<uint64_t>(B, count - off);
+            gather_f16_rows<<<blocks_for((uint64_t)rows * kIn), 256, 0, cs.s>>>(d_X.p, d_perm.p + off, rows, w.X);
+            gather_f32<<<blocks_for(rows), 256, 0, cs.s>>>(d_t.p, d_perm.p + off, rows, w.t);
+            if ((st = pass(m, w, rows, cs.s))) return st;
+            m->adam_step++;
+            const float c1 = 1.0f - std::pow(b1, (float)m->adam_step), c2 = 1.0f - std::pow(b2, (float)m->adam_step);
+            adam_kernel<<<blocks_for(kParams), 256, 0, cs.s>>>(m->params, m->grad, m->m, m->v, kParams, o.lr, b1, b2,
+                                                                eps, c1, c2, m->w1h, m->w2h);
+        }
+        float l = 0;
+        st = cuda_status(cudaMemcpyAsync(&l, w.loss, sizeof(float), cudaMemcpyDeviceToHost, cs.s));
+        if (!st) st = cuda_status(cudaStreamSynchronize(cs.s));
+        if (st) return st;
+        if (epoch_loss) epoch_loss[ep] = l / (float)count;
+    }
+    return cuda_status(cudaStreamSynchronize(cs.s));
+}
+
+}  // extern "C"
+
+namespace nqb {
+
+int model_predict_device(const nqb_model* m, const nqb_state* d_states, uint32_t count, float* d_out, cudaStream_t s) {
+    if (count == 0) return NQB_OK;
+    cudaError_t e = cudaFuncSetAttribute(predict_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPredictSmem);
+    if (e != cudaSuccess) return cuda_status(e);
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device);
+    const uint64_t tiles = (count + 63) / 64;
+    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(tiles, (uint64_t)sms * 2));
+    predict_kernel<<<grid, 128, kPredictSmem, s>>>(reinterpret_cast<const uint4*>(d_states), count, m->w1h, m->w2h,
+                                                   m->params, d_out);
+    return cuda_status(cudaGetLastError());
+}
+
+int model_device(const nqb_model* m) { return m->device; }
+
+}  // namespace nqb

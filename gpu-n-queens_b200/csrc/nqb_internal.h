@@ -37,6 +37,22 @@ int launch_batched(const nqb_state* d_items, uint32_t n_items, const uint32_t* d
                    unsigned long long* d_per_board_nodes, int block_size, unsigned stack_depth, int device,
                    cudaStream_t stream, unsigned* launches);
 
+// Batched form with optional learned scheduling (schedule.cu): with o.model, items are
+// split and ordered by predicted cost before the launch; otherwise launched as given.
+struct SchedInfo {
+    uint64_t items = 0;     // items given to the search kernel
+    double sched_ms = 0.0;  // prediction + splitting + ordering (device time)
+};
+int launch_batched_scheduled(const nqb_state* d_items, uint32_t n, const uint32_t* d_board, uint32_t* d_head,
+                             unsigned long long* d_out, unsigned long long* d_per_board,
+                             unsigned long long* d_per_board_nodes, const nqb_opts& o, unsigned stack_depth,
+                             int device, cudaStream_t s, unsigned* launches, SchedInfo* info);
+
 int cuda_status(cudaError_t e);
+
+// Learned cost model (mlp.cu): predicted log2(1 + nodes) of `count` device states.
+int model_predict_device(const nqb_model* m, const nqb_state* d_states, uint32_t count, float* d_out,
+                         cudaStream_t s);
+int model_device(const nqb_model* m);
 
 }  // namespace nqb

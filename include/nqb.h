@@ -71,15 +71,22 @@ typedef struct nqb_state {
 #define NQB_FORM_PLAIN 0   /* one thread per state, static assignment            */
 #define NQB_FORM_BATCHED 1 /* persistent kernel, device work queue, re-splitting */
 
+struct nqb_model; /* learned cost model, see nqb_model_create */
+
 typedef struct nqb_opts {
     int device;           /* CUDA device ordinal (default 0)                           */
     int form;             /* NQB_FORM_PLAIN or NQB_FORM_BATCHED                        */
     int block_size;       /* threads per block; 0 = library default                    */
     int count_unit_nodes; /* 1: also count unit-propagation placements (slower kernel) */
-    int use_model;        /* batched form: 1 = order/split with the learned model      */
-    int split_depth;      /* batched form: extra rows pre-expanded for large states;
-                             -1 = library default                                       */
-    int reserved[10];
+    int max_split_rounds; /* batched form with a model: rounds of splitting the items
+                             predicted larger than the split threshold into their
+                             children; -1 = library default (3), 0 = no splitting       */
+    int split_factor;     /* batched form with a model: split threshold = predicted total
+                             nodes / (resident lanes x split_factor); 0 = default (4)   */
+    const struct nqb_model* model; /* batched form: learned cost model; the queue is
+                             ordered largest predicted first and large items are split.
+                             NULL = FIFO: items in the given order, no splitting        */
+    int reserved[8];
 } nqb_opts;
 
 typedef struct nqb_stats {
@@ -92,7 +99,9 @@ typedef struct nqb_stats {
     double wall_ms;      /* whole call                                             */
     uint32_t pregen_depth;
     uint32_t kernel_launches;
-    uint32_t reserved[6];
+    uint64_t items;      /* items the search kernel was given (after learned splitting) */
+    double sched_ms;     /* learned scheduling: prediction, splitting, ordering        */
+    uint32_t reserved[2];
 } nqb_stats;
 
 /* Fills `opts` with the defaults (device 0, plain form, library block size). */
@@ -216,6 +225,50 @@ int nqb_plain_launch(const nqb_state* d_states, uint64_t count, uint64_t* d_out,
  */
 int nqb_batched_launch(const nqb_state* d_items, uint64_t count, const uint32_t* d_order, uint32_t* d_head,
                        uint64_t* d_out, int block_size, unsigned stack_depth, void* stream);
+
+/* ---- learned cost model ------------------------------------------------ */
+/*
+ * An MLP (NQB_MODEL_INPUTS -> 128 -> 128 -> 1, GELU) predicting log2(1 + nodes) of the
+ * search below a state, from the state's masks (free columns, both diagonals: 3 x 32
+ * bits), n/32, row/32, free columns/32 and next-row candidates/32.  Trained on the GPU by
+ * the library's own kernels (FP16 operands, FP32 accumulation, Adam) on node counts the
+ * solver records (nqb_record_nodes).  It only orders and splits the batched form's queue;
+ * counts never depend on it.  No counterpart in the reference.
+ */
+#define NQB_MODEL_INPUTS 112
+#define NQB_MODEL_PARAMS 31105 /* W1 112x128 | b1 | W2 128x128 | b2 | w3 128 | b3, row-major [in][out] */
+
+typedef struct nqb_model nqb_model;
+
+typedef struct nqb_train_opts {
+    int epochs;    /* passes over the data (default 8)  */
+    int batch;     /* rows per Adam step (default 4096)  */
+    float lr;      /* Adam learning rate (default 1e-3)  */
+    int reserved0;
+    uint64_t seed; /* shuffling seed (default 1)         */
+    int reserved[8];
+} nqb_train_opts;
+
+/* Creates a model on `device` with seeded Glorot-uniform weights. */
+int nqb_model_create(int device, uint64_t seed, nqb_model** model);
+void nqb_model_destroy(nqb_model* model);
+int nqb_model_get_params(const nqb_model* model, float* params /* NQB_MODEL_PARAMS */);
+int nqb_model_set_params(nqb_model* model, const float* params /* NQB_MODEL_PARAMS */);
+/* Host computation of the input features (count x NQB_MODEL_INPUTS floats). */
+int nqb_model_features(const nqb_state* states, uint64_t count, float* features);
+/* Predicted log2(1 + nodes) per state (fused tensor-core inference kernel). */
+int nqb_model_predict(const nqb_model* model, const nqb_state* states, uint64_t count, float* log2_nodes);
+/* One forward and backward pass over all `count` rows (count <= 2^20): mean squared
+ * error and its gradient (NQB_MODEL_PARAMS floats), without updating the weights. */
+int nqb_model_loss_grad(nqb_model* model, const nqb_state* states, const float* targets, uint64_t count,
+                        float* loss, float* grad);
+/* Trains on (state, target) pairs; epoch_loss (optional) receives each epoch's mean loss. */
+int nqb_model_train(nqb_model* model, const nqb_state* states, const float* targets, uint64_t count,
+                    const nqb_train_opts* opts, float* epoch_loss);
+/* Per-state search nodes and (weighted) completions, recorded by the batched kernel: the
+ * training labels of the cost model. */
+int nqb_record_nodes(const nqb_state* states, uint64_t count, const nqb_opts* opts, uint64_t* nodes,
+                     uint64_t* counts);
 
 /* Scratch held by nqb_batched_launch_static on every GPU that loads the library. */
 #define NQB_STATIC_SCRATCH_BYTES 256

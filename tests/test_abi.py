@@ -54,4 +54,5 @@ def test_no_device_reports_nodevice(nqb):
 
 def test_default_opts(nqb):
     o = nqb.make_opts()
-    assert (o.device, o.form, o.block_size, o.count_unit_nodes, o.split_depth) == (0, 0, 0, 0, -1)
+    assert (o.device, o.form, o.block_size, o.count_unit_nodes, o.max_split_rounds, o.split_factor) == (0, 0, 0, 0, -1, 0)
+    assert not o.model
