@@ -344,6 +344,56 @@ def model_features(states):
     return out[:len(states)]
 
 
+class BatchPlan:
+    """A board set solved repeatedly through one captured CUDA graph (nqb_batch_plan_*)."""
+
+    def __init__(self, boards, device=0, model=None, autotune=True, block_size=0, split_factor=0,
+                 max_split_rounds=-1):
+        L = lib()
+        vp = ctypes.c_void_p
+        for name, (res, args) in {
+            "nqb_batch_plan_create": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.POINTER(Opts), ctypes.c_int,
+                                                     ctypes.POINTER(vp)]),
+            "nqb_batch_plan_run": (ctypes.c_int, [vp, vp, ctypes.POINTER(Stats)]),
+            "nqb_batch_plan_config": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                                     ctypes.POINTER(ctypes.c_uint64)]),
+            "nqb_batch_plan_destroy": (None, [vp]),
+        }.items():
+            f = getattr(L, name)
+            f.restype, f.argtypes = res, args
+        self.handle = None
+        self.boards = np.ascontiguousarray(boards, dtype=STATE_DTYPE)
+        o = make_opts(device=device, form=FORM_BATCHED, block_size=block_size, model=model,
+                      max_split_rounds=max_split_rounds, split_factor=split_factor)
+        h = ctypes.c_void_p()
+        _check(L.nqb_batch_plan_create(self.boards.ctypes.data, len(self.boards), ctypes.byref(o), int(autotune),
+                                       ctypes.byref(h)), "nqb_batch_plan_create")
+        self.handle = h.value
+
+    def run(self):
+        out = np.zeros(len(self.boards), dtype=np.uint64)
+        st = Stats()
+        _check(lib().nqb_batch_plan_run(self.handle, out.ctypes.data, ctypes.byref(st)), "nqb_batch_plan_run")
+        return out, st.as_dict()
+
+    def config(self):
+        b, f, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_uint64()
+        _check(lib().nqb_batch_plan_config(self.handle, ctypes.byref(b), ctypes.byref(f), ctypes.byref(n)),
+               "nqb_batch_plan_config")
+        return {"block_size": b.value, "split_factor": f.value, "items": n.value}
+
+    def close(self):
+        if self.handle:
+            lib().nqb_batch_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def record_nodes(states, device=0):
     """(nodes, weighted counts) per state, recorded by the batched search kernel."""
     L = lib()

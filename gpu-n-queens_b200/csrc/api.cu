@@ -11,6 +11,11 @@
 
 namespace nqb {
 
+bool state_valid(const nqb_state& s) {
+    if (s.n < 1 || s.n > NQB_MAX_N || s.flags != 0) return false;
+    return (s.cols & ~board_mask(s.n)) == 0;
+}
+
 int cuda_status(cudaError_t e) {
     if (e == cudaSuccess) return NQB_OK;
     if (e == cudaErrorMemoryAllocation) return NQB_E_NOMEM;
@@ -83,10 +88,6 @@ nqb_opts resolve(const nqb_opts* o) {
     return r;
 }
 
-bool state_ok(const nqb_state& s) {
-    if (s.n < 1 || s.n > NQB_MAX_N || s.flags != 0) return false;
-    return (s.cols & ~board_mask(s.n)) == 0;
-}
 
 // Solves `count` host states on the device with the form o.form; fills totals
 // {count, nodes, unit, err} and, if per_state != nullptr, per-state weighted counts.
@@ -94,7 +95,7 @@ int solve_host_states(Scope& sc, const nqb_state* states, uint64_t count, const 
                       unsigned long long totals[4], uint64_t* per_state, nqb_stats* st,
                       uint64_t* per_state_nodes = nullptr) {
     for (uint64_t i = 0; i < count; ++i)
-        if (!state_ok(states[i])) return NQB_E_INVALID;
+        if (!state_valid(states[i])) return NQB_E_INVALID;
     const bool batched = o.form == NQB_FORM_BATCHED;
     if (o.form != NQB_FORM_PLAIN && !batched) return NQB_E_INVALID;
     if (batched && count > (1ull << 31)) return NQB_E_RANGE;

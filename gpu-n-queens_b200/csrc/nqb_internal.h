@@ -11,6 +11,9 @@ namespace nqb {
 
 inline uint32_t board_mask(unsigned n) { return n >= 32 ? 0xFFFFFFFFu : ((1u << n) - 1u); }
 
+// A state the kernels accept: 1 <= n <= 31, flags 0, no column outside the board.
+bool state_valid(const nqb_state& s);
+
 // Host pool generator (pool.cpp).  With buf == nullptr only count/weighted are computed.
 // Returns NQB_E_RANGE when the pool holds more than `capacity` states.
 int generate_pool(unsigned n, unsigned depth, nqb_state* buf, uint64_t capacity, uint64_t* count,
@@ -36,6 +39,27 @@ int launch_batched(const nqb_state* d_items, uint32_t n_items, const uint32_t* d
                    uint32_t* d_head, unsigned long long* d_out, unsigned long long* d_per_board,
                    unsigned long long* d_per_board_nodes, int block_size, unsigned stack_depth, int device,
                    cudaStream_t stream, unsigned* launches);
+
+// Items after learned scheduling: the caller's arrays, or split / ordered device copies
+// owned by the schedule until release() (stream-ordered frees).
+struct Schedule {
+    const uint4* items = nullptr;
+    const uint32_t* board = nullptr;  // item -> output slot (nullptr: identity)
+    const uint32_t* order = nullptr;  // queue order (nullptr: as stored)
+    uint32_t n = 0;
+    double sched_ms = 0.0;
+    uint4* owned_items = nullptr;
+    uint32_t* owned_board = nullptr;
+    uint32_t* owned_order = nullptr;
+    cudaStream_t stream = nullptr;
+    void release();
+};
+// Predicts, splits and orders `n` device items with o.model (no-op without a model or
+// for queues longer than 64 items per resident lane).  Split placements are added into
+// *d_split_nodes (and d_per_board_nodes[board]).
+int schedule_items(const nqb_state* d_items, uint32_t n, const uint32_t* d_board, const nqb_opts& o, int device,
+                   cudaStream_t s, unsigned long long* d_split_nodes, unsigned long long* d_per_board_nodes,
+                   Schedule* out);
 
 // Batched form with optional learned scheduling (schedule.cu): with o.model, items are
 // split and ordered by predicted cost before the launch; otherwise launched as given.

@@ -1,0 +1,239 @@
+// Batch plans: a batch of uneven partial boards solved repeatedly through one captured CUDA
+// graph, with the launch configuration chosen by timing (the autotuner).
+//
+// Creation uploads the boards once, builds the learned schedule (split + order, schedule.cu)
+// for each candidate split factor, and captures per candidate block size the whole solve
+// (zero the per-board counts and the queue head, one batched-kernel launch, read the
+// results back into pinned host memory) into a CUDA graph.  With autotuning every
+// (block size, split factor) candidate is replayed once and timed with CUDA events; the
+// fastest is kept.  A run is then a single cudaGraphLaunch.
+#include <cstring>
+#include <vector>
+
+#include "nqb_internal.h"
+
+struct nqb_batch_plan {
+    int device = 0;
+    int prev_device = 0;
+    cudaStream_t s = nullptr;
+    uint64_t count = 0;
+    unsigned stack_depth = 0;
+    nqb_state* d_boards = nullptr;
+    unsigned long long* d_per = nullptr;  // per-board weighted counts
+    unsigned long long* d_out = nullptr;  // {count, nodes, unit, error flags, queue head}
+    unsigned long long* d_split = nullptr;
+    unsigned long long* h_per = nullptr;  // pinned
+    unsigned long long* h_out = nullptr;  // pinned
+    nqb::Schedule sch;
+    uint64_t split_nodes = 0;
+    cudaGraphExec_t exec = nullptr;
+    int block = 128;
+    int factor = 0;
+    double sched_ms = 0.0;
+};
+
+namespace {
+
+using nqb::cuda_status;
+
+// Zero the outputs and the queue head, launch, read back: the sequence a run replays.
+int solve_sequence(nqb_batch_plan* p, int block) {
+    cudaStream_t s = p->s;
+    uint32_t* head = reinterpret_cast<uint32_t*>(p->d_out + 4);
+    int st = cuda_status(cudaMemsetAsync(p->d_per, 0, p->count * sizeof(unsigned long long), s));
+    if (!st) st = cuda_status(cudaMemsetAsync(p->d_out, 0, 5 * sizeof(unsigned long long), s));
+    if (!st)
+        st = nqb::launch_batched(reinterpret_cast<const nqb_state*>(p->sch.items), p->sch.n, p->sch.order,
+                                 p->sch.board, head, p->d_out, p->d_per, nullptr, block, p->stack_depth, p->device, s,
+                                 nullptr);
+    if (!st)
+        st = cuda_status(
+            cudaMemcpyAsync(p->h_per, p->d_per, p->count * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    if (!st)
+        st = cuda_status(
+            cudaMemcpyAsync(p->h_out, p->d_out, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    return st;
+}
+
+int capture(nqb_batch_plan* p, int block, cudaGraphExec_t* exec) {
+    // one uncaptured pass first: sets the kernel's attributes and checks the launch
+    int st = solve_sequence(p, block);
+    if (!st) st = cuda_status(cudaStreamSynchronize(p->s));
+    if (st) return st;
+    cudaGraph_t g = nullptr;
+    if ((st = cuda_status(cudaStreamBeginCapture(p->s, cudaStreamCaptureModeRelaxed)))) return st;
+    const int st_body = solve_sequence(p, block);
+    st = cuda_status(cudaStreamEndCapture(p->s, &g));
+    if (st_body) st = st_body;
+    if (!st) st = cuda_status(cudaGraphInstantiate(exec, g, 0));
+    if (g) cudaGraphDestroy(g);
+    return st;
+}
+
+int time_graph(nqb_batch_plan* p, cudaGraphExec_t exec, float* ms) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, p->s);
+    int st = cuda_status(cudaGraphLaunch(exec, p->s));
+    cudaEventRecord(b, p->s);
+    if (!st) st = cuda_status(cudaEventSynchronize(b));
+    if (!st) cudaEventElapsedTime(ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return st;
+}
+
+int build_schedule(nqb_batch_plan* p, const nqb_opts& o, int factor) {
+    p->sch.release();
+    p->sch = nqb::Schedule();
+    nqb_opts oo = o;
+    oo.split_factor = factor;
+    cudaMemsetAsync(p->d_split, 0, sizeof(unsigned long long), p->s);
+    int st = nqb::schedule_items(p->d_boards, (uint32_t)p->count, nullptr, oo, p->device, p->s, p->d_split, nullptr,
+                                 &p->sch);
+    unsigned long long split = 0;
+    if (!st) st = cuda_status(cudaMemcpyAsync(&split, p->d_split, sizeof(split), cudaMemcpyDeviceToHost, p->s));
+    if (!st) st = cuda_status(cudaStreamSynchronize(p->s));
+    p->split_nodes = split;
+    p->factor = factor;
+    p->sched_ms = p->sch.sched_ms;
+    return st;
+}
+
+}  // namespace
+
+extern "C" {
+
+void nqb_batch_plan_destroy(nqb_batch_plan* p) {
+    if (!p) return;
+    cudaSetDevice(p->device);
+    if (p->s) cudaStreamSynchronize(p->s);
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    p->sch.release();
+    if (p->s) cudaStreamSynchronize(p->s);
+    cudaFree(p->d_boards);
+    cudaFree(p->d_per);
+    cudaFree(p->d_out);
+    cudaFree(p->d_split);
+    cudaFreeHost(p->h_per);
+    cudaFreeHost(p->h_out);
+    if (p->s) cudaStreamDestroy(p->s);
+    cudaSetDevice(p->prev_device);
+    delete p;
+}
+
+int nqb_batch_plan_create(const nqb_state* boards, uint64_t count, const nqb_opts* opts, int autotune,
+                          nqb_batch_plan** out) {
+    if (!out || !boards || count == 0) return NQB_E_INVALID;
+    *out = nullptr;
+    if (count > (1ull << 31)) return NQB_E_RANGE;
+    nqb_opts o;
+    nqb_default_opts(&o);
+    if (opts) o = *opts;
+    for (uint64_t i = 0; i < count; ++i)
+        if (!nqb::state_valid(boards[i])) return NQB_E_INVALID;
+    int st = nqb_device_check(o.device);
+    if (st) return st;
+    nqb_batch_plan* p = new nqb_batch_plan();
+    cudaGetDevice(&p->prev_device);
+    p->device = o.device;
+    p->count = count;
+    p->stack_depth = nqb::max_stack_depth(boards, count);
+    auto fail = [&](int code) {
+        nqb_batch_plan_destroy(p);
+        return code;
+    };
+    if ((st = cuda_status(cudaSetDevice(p->device)))) return fail(st);
+    if ((st = cuda_status(cudaStreamCreateWithFlags(&p->s, cudaStreamNonBlocking)))) return fail(st);
+    if ((st = cuda_status(cudaMalloc(&p->d_boards, count * sizeof(nqb_state))))) return fail(st);
+    if ((st = cuda_status(cudaMalloc(&p->d_per, count * sizeof(unsigned long long))))) return fail(st);
+    if ((st = cuda_status(cudaMalloc(&p->d_out, 5 * sizeof(unsigned long long))))) return fail(st);
+    if ((st = cuda_status(cudaMalloc(&p->d_split, sizeof(unsigned long long))))) return fail(st);
+    if ((st = cuda_status(cudaMallocHost(&p->h_per, count * sizeof(unsigned long long))))) return fail(st);
+    if ((st = cuda_status(cudaMallocHost(&p->h_out, 4 * sizeof(unsigned long long))))) return fail(st);
+    if ((st = cuda_status(cudaMemcpyAsync(p->d_boards, boards, count * sizeof(nqb_state), cudaMemcpyHostToDevice,
+                                          p->s))))
+        return fail(st);
+
+    std::vector<int> blocks, factors;
+    if (autotune) {
+        blocks = {64, 128, 256};
+        factors = o.model ? std::vector<int>{1, 4, 16} : std::vector<int>{o.split_factor};
+    } else {
+        blocks = {o.block_size ? o.block_size : 128};
+        factors = {o.split_factor};
+    }
+    const bool timed = blocks.size() * factors.size() > 1;
+    float best = 0.0f;
+    int best_block = blocks[0], best_factor = factors[0];
+    for (int f : factors) {
+        if ((st = build_schedule(p, o, f))) return fail(st);
+        for (int b : blocks) {
+            cudaGraphExec_t ex = nullptr;
+            if ((st = capture(p, b, &ex))) return fail(st);
+            float ms = 0.0f;
+            if (timed && (st = time_graph(p, ex, &ms))) {
+                cudaGraphExecDestroy(ex);
+                return fail(st);
+            }
+            if (!p->exec || ms < best) {
+                if (p->exec) cudaGraphExecDestroy(p->exec);
+                p->exec = ex;
+                best = ms;
+                best_block = b;
+                best_factor = f;
+            } else {
+                cudaGraphExecDestroy(ex);
+            }
+        }
+    }
+    // a kept graph reads the schedule of its own split factor: rebuild both if another
+    // factor was tried after the winner
+    if (best_factor != p->factor) {
+        cudaGraphExecDestroy(p->exec);
+        p->exec = nullptr;
+        if ((st = build_schedule(p, o, best_factor))) return fail(st);
+        if ((st = capture(p, best_block, &p->exec))) return fail(st);
+    }
+    p->block = best_block;
+    *out = p;
+    cudaSetDevice(p->prev_device);
+    return NQB_OK;
+}
+
+int nqb_batch_plan_run(nqb_batch_plan* p, uint64_t* out, nqb_stats* stats) {
+    if (!p || !out) return NQB_E_INVALID;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    int st = cuda_status(cudaSetDevice(p->device));
+    float ms = 0.0f;
+    if (!st) st = time_graph(p, p->exec, &ms);
+    if (!st) {
+        std::memcpy(out, p->h_per, p->count * sizeof(uint64_t));
+        if (p->h_out[3]) st = NQB_E_DEVICE;
+    }
+    if (!st && stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->states = p->count;
+        stats->nodes = p->h_out[1] + p->split_nodes;
+        stats->unit_nodes = UINT64_MAX;
+        stats->kernel_ms = ms;
+        stats->wall_ms = ms;
+        stats->kernel_launches = 1;
+        stats->items = p->sch.n;
+        stats->sched_ms = p->sched_ms;
+    }
+    cudaSetDevice(prev);
+    return st;
+}
+
+int nqb_batch_plan_config(const nqb_batch_plan* p, int* block_size, int* split_factor, uint64_t* items) {
+    if (!p) return NQB_E_INVALID;
+    if (block_size) *block_size = p->block;
+    if (split_factor) *split_factor = p->factor;
+    if (items) *items = p->sch.n;
+    return NQB_OK;
+}
+
+}  // extern "C"

@@ -40,6 +40,11 @@ struct Buf {
         n = count;
         return cuda_status(cudaMallocAsync(reinterpret_cast<void**>(&p), (count ? count : 1) * sizeof(T), s));
     }
+    T* take() {
+        T* q = p;
+        p = nullptr;
+        return q;
+    }
     ~Buf() {
         if (p) cudaFreeAsync(p, s);
     }
@@ -111,17 +116,15 @@ __global__ void split_kernel(const uint4* __restrict__ items, const uint32_t* __
 
 }  // namespace
 
-// Runs the batched form on `n` device items.  `d_board` (optional) maps items to output
-// slots.  Extra nodes made by splitting are added into d_out[1] (and d_per_board_nodes).
-int launch_batched_scheduled(const nqb_state* d_items, uint32_t n, const uint32_t* d_board, uint32_t* d_head,
-                             unsigned long long* d_out, unsigned long long* d_per_board,
-                             unsigned long long* d_per_board_nodes, const nqb_opts& o, unsigned stack_depth,
-                             int device, cudaStream_t s, unsigned* launches, SchedInfo* info) {
-    if (info) info->items = n;
-    if (!o.model) {
-        return launch_batched(d_items, n, nullptr, d_board, d_head, d_out, d_per_board, d_per_board_nodes,
-                              o.block_size, stack_depth, device, s, launches);
-    }
+int schedule_items(const nqb_state* d_items, uint32_t n, const uint32_t* d_board, const nqb_opts& o, int device,
+                   cudaStream_t s, unsigned long long* d_split_nodes, unsigned long long* d_per_board_nodes,
+                   Schedule* out) {
+    out->items = reinterpret_cast<const uint4*>(d_items);
+    out->board = d_board;
+    out->order = nullptr;
+    out->n = n;
+    out->sched_ms = 0.0;
+    if (!o.model) return NQB_OK;
     if (model_device(o.model) != device) return NQB_E_INVALID;
     const int rounds = o.max_split_rounds < 0 ? 3 : o.max_split_rounds;
     const int factor = o.split_factor > 0 ? o.split_factor : 4;
@@ -132,10 +135,7 @@ int launch_batched_scheduled(const nqb_state* d_items, uint32_t n, const uint32_
     // fraction of the run (measured: N=21 d=7, 39M items, ordering changes nothing), so
     // the queue goes to the kernel as given; splitting likewise stops at that size.
     const uint64_t kMaxItems = (uint64_t)(64.0 * lanes);
-    if (n > kMaxItems) {
-        return launch_batched(d_items, n, nullptr, d_board, d_head, d_out, d_per_board, d_per_board_nodes,
-                              o.block_size, stack_depth, device, s, launches);
-    }
+    if (n > kMaxItems) return NQB_OK;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEventCreate(&ev0);
     cudaEventCreate(&ev1);
@@ -180,7 +180,7 @@ int launch_batched_scheduled(const nqb_state* d_items, uint32_t n, const uint32_
         const int nxt = cur == 0 ? 1 : 0;
         if ((st = items[nxt].alloc(total)) || (st = board[nxt].alloc(total))) return st;
         split_kernel<<<(n + 255) / 256, 256, 0, s>>>(cur_items, cur_board, k.p, offs.p, n, items[nxt].p,
-                                                     board[nxt].p, d_out + 1, d_per_board_nodes);
+                                                     board[nxt].p, d_split_nodes, d_per_board_nodes);
         if ((st = cuda_status(cudaGetLastError()))) return st;
         cur = nxt;
         cur_items = items[cur].p;
@@ -199,18 +199,49 @@ int launch_batched_scheduled(const nqb_state* d_items, uint32_t n, const uint32_
                                                                     (int)n, 0, 32, s))))
         return st;
     cudaEventRecord(ev1, s);
-    st = launch_batched(reinterpret_cast<const nqb_state*>(cur_items), n, order.p, cur_board, d_head, d_out,
-                        d_per_board, d_per_board_nodes, o.block_size, stack_depth, device, s, launches);
-    if (st) return st;
-    if (info) {
-        float ms = 0.0f;
-        cudaEventSynchronize(ev1);
-        cudaEventElapsedTime(&ms, ev0, ev1);
-        info->items = n;
-        info->sched_ms = ms;
+    float ms = 0.0f;
+    cudaEventSynchronize(ev1);
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    out->sched_ms = ms;
+    out->n = n;
+    out->stream = s;
+    out->owned_order = order.take();
+    out->order = out->owned_order;
+    if (cur >= 0) {
+        out->owned_items = items[cur].take();
+        out->owned_board = board[cur].take();
+        out->items = out->owned_items;
+        out->board = out->owned_board;
     }
-    // the buffers above are released on return, ordered after the kernel on the stream
     return NQB_OK;
+}
+
+void Schedule::release() {
+    if (owned_items) cudaFreeAsync(owned_items, stream);
+    if (owned_board) cudaFreeAsync(owned_board, stream);
+    if (owned_order) cudaFreeAsync(owned_order, stream);
+    owned_items = nullptr;
+    owned_board = nullptr;
+    owned_order = nullptr;
+}
+
+// Runs the batched form on `n` device items.  `d_board` (optional) maps items to output
+// slots.  Extra nodes made by splitting are added into d_out[1] (and d_per_board_nodes).
+int launch_batched_scheduled(const nqb_state* d_items, uint32_t n, const uint32_t* d_board, uint32_t* d_head,
+                             unsigned long long* d_out, unsigned long long* d_per_board,
+                             unsigned long long* d_per_board_nodes, const nqb_opts& o, unsigned stack_depth,
+                             int device, cudaStream_t s, unsigned* launches, SchedInfo* info) {
+    Schedule sch;
+    int st = schedule_items(d_items, n, d_board, o, device, s, d_out + 1, d_per_board_nodes, &sch);
+    if (!st)
+        st = launch_batched(reinterpret_cast<const nqb_state*>(sch.items), sch.n, sch.order, sch.board, d_head, d_out,
+                            d_per_board, d_per_board_nodes, o.block_size, stack_depth, device, s, launches);
+    sch.release();  // stream-ordered after the kernel that reads the arrays
+    if (info) {
+        info->items = sch.n;
+        info->sched_ms = sch.sched_ms;
+    }
+    return st;
 }
 
 }  // namespace nqb

@@ -270,6 +270,24 @@ int nqb_model_train(nqb_model* model, const nqb_state* states, const float* targ
 int nqb_record_nodes(const nqb_state* states, uint64_t count, const nqb_opts* opts, uint64_t* nodes,
                      uint64_t* counts);
 
+/* ---- batch plans: one board set solved repeatedly through a CUDA graph --- */
+/*
+ * A plan uploads `count` boards once, builds the batched form's schedule (with
+ * opts->model: learned splitting and largest-first order) and captures the solve
+ * (zeroing of the outputs, one persistent-kernel launch, read-back) into a CUDA graph.
+ * With autotune != 0 every candidate (block size 64/128/256 x split factor 1/4/16 when a
+ * model is given) is captured and timed once on the GPU and the fastest is kept.  The
+ * model is only read during creation.  No counterpart in the reference.
+ */
+typedef struct nqb_batch_plan nqb_batch_plan;
+int nqb_batch_plan_create(const nqb_state* boards, uint64_t count, const nqb_opts* opts, int autotune,
+                          nqb_batch_plan** plan);
+/* Replays the graph; out[i] = weight_i x completions of board i (as nqb_solve_batch). */
+int nqb_batch_plan_run(nqb_batch_plan* plan, uint64_t* out, nqb_stats* stats);
+/* The configuration the plan runs with. */
+int nqb_batch_plan_config(const nqb_batch_plan* plan, int* block_size, int* split_factor, uint64_t* items);
+void nqb_batch_plan_destroy(nqb_batch_plan* plan);
+
 /* Scratch held by nqb_batched_launch_static on every GPU that loads the library. */
 #define NQB_STATIC_SCRATCH_BYTES 256
 /* Largest item count nqb_batched_launch_static accepts (its 32-bit queue head). */
