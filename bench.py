@@ -257,6 +257,10 @@ def run_nqb(args):
                "gen_ms": round(float(np.mean(gen)), 3), "h2d_ms": round(float(np.mean(h2d)), 3),
                "kernel_ms": round(float(np.mean(ker)), 3), "api": "nqb_count_ex"}
 
+    extras = None
+    if rank == 0 and world == 1 and not args.skip_extras:
+        extras = run_extras(nqb, dev, args)
+
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
         rs, kind, cores = cpu_baseline_sample(n, d, args.cpu_seconds)
@@ -288,11 +292,75 @@ def run_nqb(args):
             "cpu_baseline": cpu,
             "clocks": ck,
             "gpu_launches": args.steps * (1 + (states - 1) // (1 << 30)),
+            "extras": extras,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_extras(nqb, dev, args):
+    """The learned model and the other north-star workloads, beside the headline (not timed
+    as the bench value): the cost model trained on 1M seeded N=18 prefixes (depth 4..8) with
+    node counts recorded by the solver; the 65,536 uneven partial boards solved through an
+    autotuned learned plan (CUDA graph) against the batched form without a model; the N=19
+    full count with learned scheduling against the plain and FIFO forms."""
+    out = {}
+    t0 = time.perf_counter()
+    boards = nqb.sample_boards(nqb.MODEL_SEED, args.model_samples, 18, 18, 4, 8)
+    nodes, _ = nqb.record_nodes(boards, device=dev)
+    t = np.log2(1.0 + nodes.astype(np.float64)).astype(np.float32)
+    ntr = int(0.9 * len(boards))
+    t1 = time.perf_counter()
+    model = nqb.Model(device=dev, seed=1)
+    losses = model.train(boards[:ntr], t[:ntr], epochs=8, batch=4096, lr=2e-3)
+    t2 = time.perf_counter()
+    pred = model.predict(boards[ntr:])
+    out["model"] = {"samples": len(boards), "train": ntr, "label_nodes": int(nodes.sum()),
+                    "label_s": round(t1 - t0, 2), "train_s": round(t2 - t1, 2),
+                    "epoch_loss": [round(float(x), 4) for x in losses],
+                    "val_rmse_log2": round(float(np.sqrt(np.mean((pred - t[ntr:]) ** 2))), 4),
+                    "val_std_log2": round(float(np.std(t[ntr:])), 4)}
+
+    # uneven partial boards (65,536, n 16..20, depth 3..7)
+    cb = nqb.sample_boards(nqb.BATCH_SEED, 65536, 16, 20, 3, 7)
+    fifo, st_f = nqb.solve_batch(cb, device=dev, form=nqb.FORM_BATCHED)
+    tc = time.perf_counter()
+    plan = nqb.BatchPlan(cb, device=dev, model=model, autotune=True)
+    tc = time.perf_counter() - tc
+    runs = []
+    for _ in range(3):
+        got, st_p = plan.run()
+        assert np.array_equal(got, fifo)
+        runs.append(st_p["kernel_ms"])
+    out["uneven_boards"] = {"boards": len(cb), "nodes": st_f["nodes"], "sum_counts": int(fifo.sum()),
+                            "batched_fifo_ms": round(st_f["kernel_ms"], 2), "learned_plan_ms": [round(x, 2) for x in runs],
+                            "plan": plan.config(), "plan_create_s": round(tc, 2),
+                            "learned_over_fifo": round(st_f["kernel_ms"] / min(runs), 3), "bit_exact": True}
+    plan.close()
+
+    # N=19 full counts: plain, batched FIFO, batched + learned
+    n19 = {}
+    for d in (4, 7):
+        c0, s0 = nqb.count_ex(19, d, device=dev, form=nqb.FORM_PLAIN)
+        c1, s1 = nqb.count_ex(19, d, device=dev, form=nqb.FORM_BATCHED)
+        c2, s2 = nqb.count_ex(19, d, device=dev, form=nqb.FORM_BATCHED, model=model)
+        assert c0 == c1 == c2 == KAT[19] and s0["nodes"] == s1["nodes"] == s2["nodes"]
+        n19[f"d{d}"] = {"plain_ms": round(s0["kernel_ms"], 2), "batched_ms": round(s1["kernel_ms"], 2),
+                        "learned_ms": round(s2["kernel_ms"], 2), "learned_sched_ms": round(s2["sched_ms"], 2),
+                        "learned_items": s2["items"], "learned_over_plain": round(s0["kernel_ms"] / s2["kernel_ms"], 3)}
+    pool = nqb.generate_pool(19, 5)
+    pn, _ = nqb.record_nodes(pool, device=dev)
+    pt = np.log2(1.0 + pn.astype(np.float64))
+    pp = model.predict(pool).astype(np.float64)
+    n19["rmse_log2_on_d5_pool"] = round(float(np.sqrt(np.mean((pp - pt) ** 2))), 4)
+    rank = lambda v: np.argsort(np.argsort(v)).astype(np.float64)  # ties are negligible here
+    n19["spearman_on_d5_pool"] = round(float(np.corrcoef(rank(pp), rank(pt))[0, 1]), 4)
+    n19["std_log2_on_d5_pool"] = round(float(np.std(pt)), 4)
+    out["n19"] = n19
+    model.close()
+    return out
 
 
 def run_reference(args):
@@ -356,6 +424,8 @@ def main():
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--form", default="batched", choices=["batched", "plain"])
     ap.add_argument("--skip-other-form", action="store_true")
+    ap.add_argument("--skip-extras", action="store_true")
+    ap.add_argument("--model-samples", type=int, default=1000000)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-step-seconds", type=float, default=8.0)
     ap.add_argument("--ref-cuda", type=int, default=1)

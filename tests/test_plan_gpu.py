@@ -17,10 +17,16 @@ def model(nqb):
     m.close()
 
 
-@pytest.mark.parametrize("learned,autotune", [(False, False), (False, True), (True, False), (True, True)])
-def test_plan_matches_oracle_over_replays(nqb, nqo, model, learned, autotune):
-    boards = nqb.sample_boards(4242, 6000, 10, 16, 1, 6)
+@pytest.fixture(scope="module")
+def small_batch(nqb, nqo):
+    boards = nqb.sample_boards(4242, 6000, 10, 14, 1, 6)
     want, nodes = nqo.solve_states(boards)
+    return boards, want, nodes
+
+
+@pytest.mark.parametrize("learned,autotune", [(False, False), (False, True), (True, False), (True, True)])
+def test_plan_matches_oracle_over_replays(nqb, small_batch, model, learned, autotune):
+    boards, want, nodes = small_batch
     plan = nqb.BatchPlan(boards, model=model if learned else None, autotune=autotune)
     cfg = plan.config()
     assert cfg["block_size"] in (64, 128, 256)
