@@ -6,8 +6,9 @@
 One step = one full count: every state of the depth-7 pool searched to the last row.
 `value` is search nodes/s with the pool already resident in HBM (kernel time by CUDA
 events on the launching stream); `e2e` is the same metric through the public C ABI
-call nqb_count_ex(21, 7) with host buffers: pool generation, host->device copy, kernel
-and result read-back inside the timed region.  Prints one JSON line on rank 0.
+call nqb_count_ex(21, 7) with host buffers: pool generation (on the GPU, seeded from the
+host), kernel and result read-back inside the timed region; the reference's way (pool built
+on the host and copied over, `host_pool`) is timed once beside it.  Prints one JSON line on rank 0.
 
 `--impl reference` times the reference's own CPU path (oracle/_ref, built from the
 reference's sources) on bounded stride samples of the same pool with every host core,
@@ -251,11 +252,20 @@ def run_nqb(args):
             t = torch.tensor([max(walls)], device=f"cuda:{dev}")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             wall = float(t.item())
+        # host->device: the row-0 seed states; device->host: 8 bytes of scan totals per pool
+        # level, then the 32-byte result
         e2e = {"value": nodes * world / (sum(walls) / len(walls)), "unit": "nodes/s",
-               "h2d_bytes_per_step": states * 16, "d2h_bytes_per_step": 32,
+               "h2d_bytes_per_step": 16 * ((n + 1) // 2), "d2h_bytes_per_step": 8 * d + 32,
                "wall_ms_per_step": round(1e3 * sum(walls) / len(walls), 3), "max_wall_ms": round(1e3 * wall, 3),
                "gen_ms": round(float(np.mean(gen)), 3), "h2d_ms": round(float(np.mean(h2d)), 3),
                "kernel_ms": round(float(np.mean(ker)), 3), "api": "nqb_count_ex"}
+        t0 = time.perf_counter()
+        c, st = nqb.count_ex(n, d, device=dev, form=form, host_pool=True)
+        hw = time.perf_counter() - t0
+        assert c == count
+        e2e["host_pool"] = {"wall_ms": round(1e3 * hw, 3), "gen_ms": round(st["gen_ms"], 3),
+                            "h2d_ms": round(st["h2d_ms"], 3), "h2d_bytes": states * 16,
+                            "nodes_per_s": round(nodes / hw, 1)}
 
     extras = None
     if rank == 0 and world == 1 and not args.skip_extras:

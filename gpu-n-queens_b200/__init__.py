@@ -36,7 +36,8 @@ class NQBError(RuntimeError):
 class Opts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("form", ctypes.c_int), ("block_size", ctypes.c_int),
                 ("count_unit_nodes", ctypes.c_int), ("max_split_rounds", ctypes.c_int),
-                ("split_factor", ctypes.c_int), ("model", ctypes.c_void_p), ("reserved", ctypes.c_int * 8)]
+                ("split_factor", ctypes.c_int), ("model", ctypes.c_void_p), ("host_pool", ctypes.c_int),
+                ("reserved", ctypes.c_int * 7)]
 
 
 class Stats(ctypes.Structure):
@@ -118,12 +119,13 @@ def _check(status, what):
 
 
 def make_opts(device=0, form=FORM_PLAIN, block_size=0, count_unit_nodes=False, model=None, max_split_rounds=-1,
-              split_factor=0):
+              split_factor=0, host_pool=False):
     o = Opts()
     lib().nqb_default_opts(ctypes.byref(o))
     o.device, o.form, o.block_size = device, form, block_size
     o.count_unit_nodes, o.max_split_rounds, o.split_factor = int(count_unit_nodes), max_split_rounds, split_factor
     o.model = model.handle if model is not None else None
+    o.host_pool = int(host_pool)
     return o
 
 
@@ -167,6 +169,23 @@ def generate_pool(n, depth):
     got = ctypes.c_uint64(0)
     _check(lib().nqb_generate_pool_into(n, depth, out.ctypes.data, cnt, ctypes.byref(got)), "nqb_generate_pool_into")
     return out[:got.value]
+
+
+def generate_pool_device(n, depth):
+    """The pool built on the GPU (nqb_generate_pool_device_into), returned as a numpy array."""
+    import torch
+    L = lib()
+    vp = ctypes.c_void_p
+    f = L.nqb_generate_pool_device_into
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_uint, ctypes.c_uint, vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64), vp]
+    cap = pool_size(n, depth)
+    buf = torch.empty(max(cap, 1) * 16, dtype=torch.uint8, device="cuda")
+    c = ctypes.c_uint64(0)
+    _check(f(n, depth, buf.data_ptr(), cap, ctypes.byref(c), torch.cuda.current_stream().cuda_stream),
+           "nqb_generate_pool_device_into")
+    torch.cuda.synchronize()
+    return buf[:16 * c.value].cpu().numpy().view(STATE_DTYPE)
 
 
 def generate_pool_alloc(n, depth):

@@ -89,21 +89,17 @@ nqb_opts resolve(const nqb_opts* o) {
 }
 
 
-// Solves `count` host states on the device with the form o.form; fills totals
-// {count, nodes, unit, err} and, if per_state != nullptr, per-state weighted counts.
-int solve_host_states(Scope& sc, const nqb_state* states, uint64_t count, const nqb_opts& o,
-                      unsigned long long totals[4], uint64_t* per_state, nqb_stats* st,
-                      uint64_t* per_state_nodes = nullptr) {
-    for (uint64_t i = 0; i < count; ++i)
-        if (!state_valid(states[i])) return NQB_E_INVALID;
+// Solves `count` states already on the device (d_states, stack bound `depth`) with the form
+// o.form; fills totals {count, nodes, unit, err} and optional per-state results.  e_start is
+// recorded before any H2D copy so that h2d_ms covers it.
+int solve_device_states(Scope& sc, const nqb_state* d_states, uint64_t count, unsigned depth, const nqb_opts& o,
+                        unsigned long long totals[4], uint64_t* per_state, nqb_stats* st,
+                        uint64_t* per_state_nodes, cudaEvent_t e_start) {
     const bool batched = o.form == NQB_FORM_BATCHED;
     if (o.form != NQB_FORM_PLAIN && !batched) return NQB_E_INVALID;
     if (batched && count > (1ull << 31)) return NQB_E_RANGE;
-    const unsigned depth = max_stack_depth(states, count);
-    nqb_state* d_states = nullptr;
     unsigned long long* d_out = nullptr;  // 4 result words, then the queue head
     unsigned long long* d_per = nullptr;
-    NQB_TRY(sc.alloc(&d_states, count * sizeof(nqb_state)));
     NQB_TRY(sc.alloc(&d_out, 5 * sizeof(unsigned long long)));
     if (per_state) NQB_TRY(sc.alloc(&d_per, count * sizeof(unsigned long long)));
     unsigned long long* d_per_nodes = nullptr;
@@ -113,25 +109,23 @@ int solve_host_states(Scope& sc, const nqb_state* states, uint64_t count, const 
         NQB_TRY(cuda_status(cudaMemsetAsync(d_per_nodes, 0, count * sizeof(unsigned long long), sc.stream)));
     }
     uint32_t* d_head = reinterpret_cast<uint32_t*>(d_out + 4);
-    cudaEvent_t e0, e1, e2;
-    NQB_TRY(sc.event(&e0));
+    cudaEvent_t e1, e2;
     NQB_TRY(sc.event(&e1));
     NQB_TRY(sc.event(&e2));
-    NQB_TRY(cuda_status(cudaEventRecord(e0, sc.stream)));
-    NQB_TRY(cuda_status(
-        cudaMemcpyAsync(d_states, states, count * sizeof(nqb_state), cudaMemcpyHostToDevice, sc.stream)));
     NQB_TRY(cuda_status(cudaMemsetAsync(d_out, 0, 5 * sizeof(unsigned long long), sc.stream)));
     if (d_per) NQB_TRY(cuda_status(cudaMemsetAsync(d_per, 0, count * sizeof(unsigned long long), sc.stream)));
     NQB_TRY(cuda_status(cudaEventRecord(e1, sc.stream)));
     unsigned launches = 0;
     SchedInfo sched;
     sched.items = count;
-    if (batched) {
-        NQB_TRY(launch_batched_scheduled(d_states, (uint32_t)count, nullptr, d_head, d_out, d_per, d_per_nodes, o,
-                                         depth, sc.device, sc.stream, &launches, &sched));
-    } else {
-        NQB_TRY(launch_plain(d_states, count, d_out, d_per, o.block_size, o.count_unit_nodes != 0, depth,
-                             sc.stream, &launches));
+    if (count) {
+        if (batched) {
+            NQB_TRY(launch_batched_scheduled(d_states, (uint32_t)count, nullptr, d_head, d_out, d_per, d_per_nodes, o,
+                                             depth, sc.device, sc.stream, &launches, &sched));
+        } else {
+            NQB_TRY(launch_plain(d_states, count, d_out, d_per, o.block_size, o.count_unit_nodes != 0, depth,
+                                 sc.stream, &launches));
+        }
     }
     NQB_TRY(cuda_status(cudaEventRecord(e2, sc.stream)));
     NQB_TRY(cuda_status(cudaMemcpyAsync(totals, d_out, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
@@ -146,7 +140,7 @@ int solve_host_states(Scope& sc, const nqb_state* states, uint64_t count, const 
     if (totals[3]) return NQB_E_DEVICE;
     if (st) {
         float h2d = 0, ker = 0;
-        cudaEventElapsedTime(&h2d, e0, e1);
+        if (e_start) cudaEventElapsedTime(&h2d, e_start, e1);
         cudaEventElapsedTime(&ker, e1, e2);
         st->states = count;
         st->nodes = totals[1];
@@ -158,6 +152,24 @@ int solve_host_states(Scope& sc, const nqb_state* states, uint64_t count, const 
         st->sched_ms = sched.sched_ms;
     }
     return NQB_OK;
+}
+
+// Solves `count` host states on the device with the form o.form; fills totals
+// {count, nodes, unit, err} and, if per_state != nullptr, per-state weighted counts.
+int solve_host_states(Scope& sc, const nqb_state* states, uint64_t count, const nqb_opts& o,
+                      unsigned long long totals[4], uint64_t* per_state, nqb_stats* st,
+                      uint64_t* per_state_nodes = nullptr) {
+    for (uint64_t i = 0; i < count; ++i)
+        if (!state_valid(states[i])) return NQB_E_INVALID;
+    const unsigned depth = max_stack_depth(states, count);
+    nqb_state* d_states = nullptr;
+    NQB_TRY(sc.alloc(&d_states, count * sizeof(nqb_state)));
+    cudaEvent_t e0;
+    NQB_TRY(sc.event(&e0));
+    NQB_TRY(cuda_status(cudaEventRecord(e0, sc.stream)));
+    NQB_TRY(cuda_status(
+        cudaMemcpyAsync(d_states, states, count * sizeof(nqb_state), cudaMemcpyHostToDevice, sc.stream)));
+    return solve_device_states(sc, d_states, count, depth, o, totals, per_state, st, per_state_nodes, e0);
 }
 
 void* aligned_host_alloc(size_t bytes) {
@@ -250,15 +262,34 @@ int nqb_count_ex(unsigned n, unsigned depth, const nqb_opts* opts, uint64_t* cou
     if (stats) std::memset(stats, 0, sizeof(*stats));
     Scope sc(o.device);
     NQB_TRY(sc.status);
-    nqb_state* pool = nullptr;
-    uint64_t cnt = 0;
-    const double tg = now_ms();
-    NQB_TRY(nqb_generate_pool(n, depth, &pool, &cnt));
-    const double gen_ms = now_ms() - tg;
     unsigned long long totals[4] = {0, 0, 0, 0};
-    const int s = solve_host_states(sc, pool, cnt, o, totals, nullptr, stats);
-    std::free(pool);
-    NQB_TRY(s);
+    double gen_ms = 0.0;
+    if (o.host_pool) {  // the reference's way: build the pool on the host, copy it over
+        nqb_state* pool = nullptr;
+        uint64_t cnt = 0;
+        const double tg = now_ms();
+        NQB_TRY(nqb_generate_pool(n, depth, &pool, &cnt));
+        gen_ms = now_ms() - tg;
+        const int s = solve_host_states(sc, pool, cnt, o, totals, nullptr, stats);
+        std::free(pool);
+        NQB_TRY(s);
+    } else {  // build the pool on the GPU: nothing crosses PCIe but the result
+        cudaEvent_t g0, g1;
+        NQB_TRY(sc.event(&g0));
+        NQB_TRY(sc.event(&g1));
+        NQB_TRY(cuda_status(cudaEventRecord(g0, sc.stream)));
+        nqb_state* d_pool = nullptr;
+        uint64_t cnt = 0;
+        NQB_TRY(generate_pool_device(n, depth, sc.stream, &d_pool, &cnt));
+        cudaEventRecord(g1, sc.stream);
+        const int s = solve_device_states(sc, d_pool, cnt, n - depth - 1 > 0 ? n - depth - 1 : 1, o, totals, nullptr,
+                                          stats, nullptr, nullptr);
+        cudaFreeAsync(d_pool, sc.stream);
+        NQB_TRY(s);
+        float g = 0.0f;
+        cudaEventElapsedTime(&g, g0, g1);
+        gen_ms = g;
+    }
     *count = totals[0];
     if (stats) {
         stats->gen_ms = gen_ms;
@@ -375,6 +406,28 @@ int nqb_batched_launch(const nqb_state* d_items, uint64_t count, const uint32_t*
     return launch_batched(d_items, (uint32_t)count, d_order, nullptr, d_head,
                           reinterpret_cast<unsigned long long*>(d_out), nullptr, nullptr, block_size, stack_depth, dev,
                           static_cast<cudaStream_t>(stream), nullptr);
+}
+
+int nqb_generate_pool_device(unsigned n, unsigned depth, nqb_state** d_states, uint64_t* count, void* stream) {
+    if (!d_states || !count) return NQB_E_INVALID;
+    return generate_pool_device(n, depth, static_cast<cudaStream_t>(stream), d_states, count);
+}
+
+int nqb_generate_pool_device_into(unsigned n, unsigned depth, nqb_state* d_buf, uint64_t capacity, uint64_t* count,
+                                  void* stream) {
+    if (!count || (capacity && !d_buf)) return NQB_E_INVALID;
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    nqb_state* d_pool = nullptr;
+    int s = generate_pool_device(n, depth, st, &d_pool, count);
+    if (s) return s;
+    if (*count > capacity) s = NQB_E_RANGE;
+    else if (*count) s = cuda_status(cudaMemcpyAsync(d_buf, d_pool, *count * sizeof(nqb_state), cudaMemcpyDeviceToDevice, st));
+    cudaFreeAsync(d_pool, st);
+    return s;
+}
+
+void nqb_free_device(void* p, void* stream) {
+    if (p) cudaFreeAsync(p, static_cast<cudaStream_t>(stream));
 }
 
 }  // extern "C"

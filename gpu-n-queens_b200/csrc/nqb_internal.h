@@ -19,6 +19,9 @@ bool state_valid(const nqb_state& s);
 int generate_pool(unsigned n, unsigned depth, nqb_state* buf, uint64_t capacity, uint64_t* count,
                   uint64_t* weighted);
 
+// The same pool built on the device (pool_gpu.cu), stream-ordered buffer in *d_out.
+int generate_pool_device(unsigned n, unsigned depth, cudaStream_t s, nqb_state** d_out, uint64_t* count);
+
 // Worker threads used by host-side passes (NQB_THREADS overrides the core count).
 unsigned host_threads();
 

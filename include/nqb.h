@@ -86,7 +86,9 @@ typedef struct nqb_opts {
     const struct nqb_model* model; /* batched form: learned cost model; the queue is
                              ordered largest predicted first and large items are split.
                              NULL = FIFO: items in the given order, no splitting        */
-    int reserved[8];
+    int host_pool;        /* nqb_count_ex: 1 = build the pool on the host and copy it to
+                             the GPU (the reference's way); 0 = build it on the GPU    */
+    int reserved[7];
 } nqb_opts;
 
 typedef struct nqb_stats {
@@ -145,6 +147,17 @@ int nqb_generate_pool(unsigned n, unsigned depth, nqb_state** states, uint64_t* 
  * size is computed.  Returns NQB_E_RANGE if the pool does not fit. */
 int nqb_generate_pool_into(unsigned n, unsigned depth, nqb_state* buf, uint64_t capacity,
                            uint64_t* count);
+
+/* Same pool built on the GPU (level-by-level expansion, same order), in a device buffer
+ * allocated by the library on `stream` (a cudaStream_t; stream-ordered allocation):
+ * release it with nqb_free_device.  *count may be 0.  Asynchronous apart from the level
+ * sizes it reads back. */
+int nqb_generate_pool_device(unsigned n, unsigned depth, nqb_state** d_states, uint64_t* count, void* stream);
+void nqb_free_device(void* d_ptr, void* stream);
+/* Same, copied into a caller device buffer of `capacity` states (NQB_E_RANGE, with *count
+ * set, when it does not fit). */
+int nqb_generate_pool_device_into(unsigned n, unsigned depth, nqb_state* d_buf, uint64_t capacity, uint64_t* count,
+                                  void* stream);
 
 /* Sum of the pool's weights: the number of full-board prefixes it stands for. */
 int nqb_pool_weighted_size(unsigned n, unsigned depth, uint64_t* weighted);

@@ -139,3 +139,27 @@ def test_count_17_5_config2(nqb):
     c, st = nqb.count_ex(17, 5)
     assert c == 95815104
     assert st["states"] == 114434 and st["nodes"] == 4275902721
+
+
+@pytest.mark.parametrize("n", [4, 8, 11, 13, 16, 19])
+def test_device_pool_equals_host_pool(nqb, n):
+    depths = {1, 2, n // 2, n - 2, n - 1} if n <= 16 else {1, 2, 5, 7, 9}  # deep N=19 pools hold billions
+    for d in sorted(depths):
+        if 1 <= d < n:
+            assert nqb.generate_pool_device(n, d).tobytes() == nqb.generate_pool(n, d).tobytes(), (n, d)
+
+
+def test_device_pool_large(nqb):
+    p = nqb.generate_pool_device(21, 7)
+    assert len(p) == 39430182 and int(p["weight"].sum()) == 75580634
+    h = nqb.generate_pool(21, 7)
+    assert p.tobytes() == h.tobytes()
+
+
+@pytest.mark.parametrize("form", [0, 1])
+def test_count_with_host_or_device_pool(nqb, form):
+    for n, d in [(12, 3), (16, 5), (17, 4)]:
+        c_dev, s_dev = nqb.count_ex(n, d, form=form)
+        c_host, s_host = nqb.count_ex(n, d, form=form, host_pool=True)
+        assert c_dev == c_host == KAT[n] and s_dev["nodes"] == s_host["nodes"]
+        assert s_dev["h2d_ms"] == 0.0 and s_dev["states"] == s_host["states"]
