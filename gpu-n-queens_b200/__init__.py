@@ -22,7 +22,10 @@ STATE_DTYPE = np.dtype([("cols", "<u4"), ("ldiag", "<u4"), ("rdiag", "<u4"),
                         ("row", "u1"), ("n", "u1"), ("weight", "u1"), ("flags", "u1")])
 assert STATE_DTYPE.itemsize == 16
 
-OK, E_INVALID, E_NOMEM, E_CUDA, E_NODEVICE, E_RANGE, E_STALL, E_DEVICE, E_MODEL = range(9)
+OK, E_INVALID, E_NOMEM, E_CUDA, E_NODEVICE, E_RANGE, E_STALL, E_DEVICE, E_MODEL, E_IO, E_FORMAT = range(11)
+PLACEMENT_DTYPE = np.dtype([("n", "u1"), ("row", "u1"), ("col", "u1", (30,))])
+assert PLACEMENT_DTYPE.itemsize == 32
+STATE_FILE_VERSION, STATE_FILE_FLAGS = 1, 3
 FORM_PLAIN, FORM_BATCHED = 0, 1
 MIN_N, MAX_N = 4, 31
 
@@ -97,6 +100,13 @@ def lib():
                                                 ctypes.c_uint, vp]),
             "nqb_batched_launch": (ctypes.c_int, [vp, ctypes.c_uint64, vp, vp, vp, ctypes.c_int, ctypes.c_uint,
                                                   vp]),
+            "nqb_generate_pool_placements": (ctypes.c_int, [ctypes.c_uint, ctypes.c_uint, ctypes.POINTER(vp), u64p]),
+            "nqb_states_from_placements": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.c_int, vp]),
+            "nqb_write_state_file": (ctypes.c_int, [ctypes.c_char_p, vp, ctypes.c_uint64, ctypes.c_uint,
+                                                    ctypes.c_uint, ctypes.c_int]),
+            "nqb_read_state_file": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_uint,
+                                                   ctypes.POINTER(StateFileInfo), ctypes.POINTER(vp)]),
+            "nqb_pool_for_target": (ctypes.c_int, [ctypes.c_uint, ctypes.c_uint64, ctypes.POINTER(Target)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -186,6 +196,68 @@ def generate_pool_device(n, depth):
            "nqb_generate_pool_device_into")
     torch.cuda.synchronize()
     return buf[:16 * c.value].cpu().numpy().view(STATE_DTYPE)
+
+
+def _take(ptr, nbytes):
+    """Copies a library allocation into Python bytes and releases it with nqb_free."""
+    try:
+        return bytes((ctypes.c_uint8 * nbytes).from_address(ptr.value)) if nbytes else b""
+    finally:
+        lib().nqb_free(ptr)
+
+
+def generate_pool_placements(n, depth):
+    """The (n, depth) pool as placements (PLACEMENT_DTYPE), same states and order as generate_pool."""
+    p = ctypes.c_void_p()
+    c = ctypes.c_uint64(0)
+    _check(lib().nqb_generate_pool_placements(n, depth, ctypes.byref(p), ctypes.byref(c)),
+           "nqb_generate_pool_placements")
+    return np.frombuffer(_take(p, 32 * c.value), dtype=PLACEMENT_DTYPE).copy()
+
+
+def states_from_placements(placements, mirror_weight=True):
+    pl = np.ascontiguousarray(placements, dtype=PLACEMENT_DTYPE)
+    out = np.zeros(max(len(pl), 1), dtype=STATE_DTYPE)
+    _check(lib().nqb_states_from_placements(pl.ctypes.data, len(pl), int(mirror_weight), out.ctypes.data),
+           "nqb_states_from_placements")
+    return out[:len(pl)]
+
+
+class StateFileInfo(ctypes.Structure):
+    _fields_ = [("version", ctypes.c_uint32), ("flags", ctypes.c_uint64), ("n", ctypes.c_uint),
+                ("locked_row", ctypes.c_uint), ("count", ctypes.c_uint64)]
+
+
+def write_state_file(path, placements, n, locked_row, header=True):
+    pl = np.ascontiguousarray(placements, dtype=PLACEMENT_DTYPE)
+    _check(lib().nqb_write_state_file(os.fsencode(path), pl.ctypes.data, len(pl), n, locked_row, int(header)),
+           f"nqb_write_state_file({path})")
+
+
+def read_state_file(path, header=True, expect_n=0):
+    """(info dict, placements) of a .nqsf state file."""
+    info = StateFileInfo()
+    p = ctypes.c_void_p()
+    _check(lib().nqb_read_state_file(os.fsencode(path), int(header), expect_n, ctypes.byref(info), ctypes.byref(p)),
+           f"nqb_read_state_file({path})")
+    pl = np.frombuffer(_take(p, 32 * info.count), dtype=PLACEMENT_DTYPE).copy()
+    return {k: getattr(info, k) for k, _ in StateFileInfo._fields_}, pl
+
+
+class Target(ctypes.Structure):
+    _fields_ = [("lock_row", ctypes.c_uint), ("pool_depth", ctypes.c_uint), ("count", ctypes.c_uint64),
+                ("hard_limit", ctypes.c_uint64), ("first_row", ctypes.c_uint), ("tried", ctypes.c_uint),
+                ("limit_hit", ctypes.c_int), ("reserved", ctypes.c_uint), ("tried_count", ctypes.c_uint64 * 32)]
+
+
+def pool_for_target(n, how_many):
+    """Count-target sizing: dict with lock_row, pool_depth, count, hard_limit, first_row, tried rows."""
+    t = Target()
+    _check(lib().nqb_pool_for_target(n, ctypes.c_uint64(how_many), ctypes.byref(t)),
+           f"nqb_pool_for_target({n}, {how_many})")
+    d = {k: getattr(t, k) for k, _ in Target._fields_ if k not in ("reserved", "tried_count")}
+    d["tried_count"] = list(t.tried_count[:t.tried])
+    return d
 
 
 def generate_pool_alloc(n, depth):

@@ -75,12 +75,6 @@ class Scope {
     std::vector<cudaEvent_t> events_;
 };
 
-#define NQB_TRY(expr)                   \
-    do {                                \
-        const int s_ = (expr);          \
-        if (s_ != NQB_OK) return s_;    \
-    } while (0)
-
 nqb_opts resolve(const nqb_opts* o) {
     nqb_opts r;
     nqb_default_opts(&r);
@@ -207,6 +201,8 @@ const char* nqb_strerror(int s) {
         case NQB_E_STALL: return "device-side bounded wait ran out";
         case NQB_E_DEVICE: return "device-side check failed";
         case NQB_E_MODEL: return "learned cost model missing or not trained";
+        case NQB_E_IO: return "file could not be opened, read or written";
+        case NQB_E_FORMAT: return "malformed state file, or another version or generation flags";
         default: return "unknown status";
     }
 }

@@ -7,6 +7,13 @@
 
 #include "nqb.h"
 
+// Returns from the enclosing function with the status of `expr` unless it is NQB_OK.
+#define NQB_TRY(expr)                \
+    do {                             \
+        const int s_ = (expr);       \
+        if (s_ != NQB_OK) return s_; \
+    } while (0)
+
 namespace nqb {
 
 inline uint32_t board_mask(unsigned n) { return n >= 32 ? 0xFFFFFFFFu : ((1u << n) - 1u); }
@@ -16,6 +23,11 @@ bool state_valid(const nqb_state& s);
 
 // Host pool generator (pool.cpp).  With buf == nullptr only count/weighted are computed.
 // Returns NQB_E_RANGE when the pool holds more than `capacity` states.
+// Host generator with optional outputs: states (buf), placements (pbuf), the pool size
+// of each row-0 column (per_first_col, ceil(n/2) entries).  With buf and pbuf both null
+// only the sizes are computed.
+int generate_pool_ex(unsigned n, unsigned depth, nqb_state* buf, nqb_placement* pbuf, uint64_t capacity,
+                     uint64_t* count, uint64_t* weighted, uint64_t* per_first_col);
 int generate_pool(unsigned n, unsigned depth, nqb_state* buf, uint64_t capacity, uint64_t* count,
                   uint64_t* weighted);
 

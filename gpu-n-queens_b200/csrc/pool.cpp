@@ -11,6 +11,7 @@
 // place, so the concatenated order equals the reference's.
 #include <algorithm>
 #include <atomic>
+#include <cstring>
 #include <cstdlib>
 #include <thread>
 #include <vector>
@@ -34,12 +35,21 @@ struct Walker {
     unsigned n, depth;
     uint32_t mask;
     uint8_t weight;
-    nqb_state* out;  // nullptr: count only
+    nqb_state* out;      // nullptr: no states written
+    nqb_placement* pout; // nullptr: no placements written
     uint64_t cnt = 0;
+    uint8_t path[32];    // column of the queen in each row placed so far
 
     void walk(unsigned row, uint32_t cols, uint32_t ld, uint32_t rd) {
         if (row == depth) {
             if (mask & ~(cols | ld | rd)) {
+                if (pout) {
+                    nqb_placement& p = pout[cnt];
+                    std::memset(&p, 0xFF, sizeof(p));  // rows >= depth: no queen (UNSET)
+                    p.n = (uint8_t)n;
+                    p.row = (uint8_t)row;
+                    std::memcpy(p.col, path, row);
+                }
                 if (out) {
                     nqb_state& s = out[cnt];
                     s.cols = cols;
@@ -58,6 +68,7 @@ struct Walker {
         while (f) {
             const uint32_t b = f & (0u - f);
             f ^= b;
+            path[row] = (uint8_t)__builtin_ctz(b);
             walk(row + 1, cols | b, (ld | b) << 1, (rd | b) >> 1);
         }
     }
@@ -70,8 +81,8 @@ struct Task {
 
 }  // namespace
 
-int generate_pool(unsigned n, unsigned depth, nqb_state* buf, uint64_t capacity, uint64_t* count,
-                  uint64_t* weighted) {
+int generate_pool_ex(unsigned n, unsigned depth, nqb_state* buf, nqb_placement* pbuf, uint64_t capacity,
+                     uint64_t* count, uint64_t* weighted, uint64_t* per_first_col) {
     if (n < NQB_MIN_N || n > NQB_MAX_N || depth < 1 || depth >= n || !count) return NQB_E_INVALID;
     const uint32_t mask = board_mask(n);
     const unsigned half = (n + 1) / 2;  // row-0 columns searched (mirror elimination)
@@ -90,21 +101,20 @@ int generate_pool(unsigned n, unsigned depth, nqb_state* buf, uint64_t capacity,
             tasks.push_back({c0, __builtin_ctz(b1)});
         }
     }
-    auto make_walker = [&](const Task& t, nqb_state* out) {
+    auto run_task = [&](const Task& t, nqb_state* out, nqb_placement* pout) -> uint64_t {
         Walker w;
         w.n = n;
         w.depth = depth;
         w.mask = mask;
         w.weight = (uint8_t)(t.c0 < (n >> 1) ? 2 : 1);  // GPU_NQueens.cu:354-357
         w.out = out;
-        return w;
-    };
-    auto run_task = [&](const Task& t, nqb_state* out) -> uint64_t {
-        Walker w = make_walker(t, out);
+        w.pout = pout;
+        w.path[0] = (uint8_t)t.c0;
         const uint32_t b0 = 1u << t.c0;
         if (t.c1 < 0) {
             w.walk(1, b0, b0 << 1, b0 >> 1);
         } else {
+            w.path[1] = (uint8_t)t.c1;
             const uint32_t b1 = 1u << t.c1;
             const uint32_t ld = ((b0 << 1) | b1) << 1, rd = ((b0 >> 1) | b1) >> 1;
             w.walk(2, b0 | b1, ld, rd);
@@ -132,7 +142,7 @@ int generate_pool(unsigned n, unsigned depth, nqb_state* buf, uint64_t capacity,
         for (unsigned i = 0; i < nt; ++i) ts.emplace_back(body);
         for (auto& t : ts) t.join();
     };
-    parallel([&](size_t k) { sizes[k] = run_task(tasks[k], nullptr); });
+    parallel([&](size_t k) { sizes[k] = run_task(tasks[k], nullptr, nullptr); });
 
     std::vector<uint64_t> offs(tasks.size() + 1, 0);
     uint64_t w_total = 0;
@@ -142,10 +152,19 @@ int generate_pool(unsigned n, unsigned depth, nqb_state* buf, uint64_t capacity,
     }
     *count = offs.back();
     if (weighted) *weighted = w_total;
-    if (!buf) return NQB_OK;
+    if (per_first_col) {
+        std::fill(per_first_col, per_first_col + half, 0ull);
+        for (size_t k = 0; k < tasks.size(); ++k) per_first_col[tasks[k].c0] += sizes[k];
+    }
+    if (!buf && !pbuf) return NQB_OK;
     if (offs.back() > capacity) return NQB_E_RANGE;
-    parallel([&](size_t k) { run_task(tasks[k], buf + offs[k]); });
+    parallel([&](size_t k) { run_task(tasks[k], buf ? buf + offs[k] : nullptr, pbuf ? pbuf + offs[k] : nullptr); });
     return NQB_OK;
+}
+
+int generate_pool(unsigned n, unsigned depth, nqb_state* buf, uint64_t capacity, uint64_t* count,
+                  uint64_t* weighted) {
+    return generate_pool_ex(n, depth, buf, nullptr, capacity, count, weighted, nullptr);
 }
 
 unsigned max_stack_depth(const nqb_state* states, uint64_t count) {

@@ -39,6 +39,9 @@ extern "C" {
 #define NQB_E_STALL 6    /* a device-side bounded wait ran out                    */
 #define NQB_E_DEVICE 7   /* a device-side bounds check failed                     */
 #define NQB_E_MODEL 8    /* learned cost model missing or not trained            */
+#define NQB_E_IO 9       /* a file could not be opened, read or written          */
+#define NQB_E_FORMAT 10  /* a state file is malformed, or of another version or
+                            generation flags (reference reader: -3 / -4)          */
 
 /* ---- search state ------------------------------------------------------ */
 /*
@@ -158,6 +161,88 @@ void nqb_free_device(void* d_ptr, void* stream);
  * set, when it does not fit). */
 int nqb_generate_pool_device_into(unsigned n, unsigned depth, nqb_state* d_buf, uint64_t capacity, uint64_t* count,
                                   void* stream);
+
+/* ---- placements, state files and count-target sizing ----------------- */
+/*
+ * A partial board as the reference's state files hold it: the column of the queen in
+ * each row [0, row) (nq_state_t.queen_at_index / curr_row, n_queens.cuh:100-113);
+ * col[r] for r >= row is 0xFF (the reference's UNSET_QUEEN_INDEX).  32 bytes.
+ */
+typedef struct nqb_placement {
+    uint8_t n;
+    uint8_t row;
+    uint8_t col[30];
+} nqb_placement;
+
+/* The pool of nqb_generate_pool as placements, same states in the same order;
+ * release with nqb_free. */
+int nqb_generate_pool_placements(unsigned n, unsigned depth, nqb_placement** placements, uint64_t* count);
+
+/* Rebuilds search states from placements by placing each queen in turn (the state-file
+ * reader's place_queen_at loop, nq_utils.cu:232-240).  mirror_weight != 0: weight 2 when
+ * the row-0 queen is left of centre, else 1 (GPU_NQueens.cu:354-357); 0: weight 1.
+ * NQB_E_INVALID for n out of range, row >= n or row > 30, or a column >= n. */
+int nqb_states_from_placements(const nqb_placement* placements, uint64_t count, int mirror_weight, nqb_state* out);
+
+/* State files (.nqsf; nq_utils.cu:127-259).  Layout, little-endian:
+ *   [u32 version = 1, u64 flags]   generation-flags header (COMPILATION_PARAMETER_FLAGS_
+ *                                  IN_STATE_FILES, on in the reference's default build)
+ *   u8 n, u8 locked_row, u64 total
+ *   per distinct row r, ascending: u8 r, u64 cnt, then cnt x r column bytes, the states
+ *   of that row in input order.
+ * flags: bit 0 experimental optimisations, bit 1 mirror elimination; the reference's
+ * default build, and this library, write NQB_STATE_FILE_FLAGS. */
+#define NQB_STATE_FILE_VERSION 1
+#define NQB_STATE_FILE_FLAGS 3ull
+
+typedef struct nqb_state_file {
+    uint32_t version;    /* 0 when the file has no header                          */
+    uint64_t flags;
+    unsigned n;
+    unsigned locked_row;
+    uint64_t count;
+} nqb_state_file;
+
+/* Writes `count` placements (all of board size n) with the given locked row.  count == 0
+ * is NQB_E_INVALID, as the reference writer refuses an empty buffer.  header != 0 writes
+ * the version/flags header. */
+int nqb_write_state_file(const char* path, const nqb_placement* placements, uint64_t count, unsigned n,
+                         unsigned locked_row, int header);
+
+/* Reads a state file.  expect_n != 0 requires that board size (the reference asserts
+ * it).  With a header, version != 1 or flags != NQB_STATE_FILE_FLAGS is NQB_E_FORMAT
+ * (the reference returns -3 / -4); so is a truncated file, a segment row >= n, a column
+ * >= n, or segment counts that do not add up to the total.  *placements is allocated by
+ * the library (release with nqb_free) and *info filled. */
+int nqb_read_state_file(const char* path, int header, unsigned expect_n, nqb_state_file* info,
+                        nqb_placement** placements);
+
+/*
+ * Count-target pool sizing (nq_generate_states -> gen_states_threaded, n_queens.cu:128-219,
+ * :397-406; deffinitions.cuh:57,61): the lock row the reference picks for a requested
+ * pool size `how_many`.  Hard limit = (uint64)(how_many * 1.2); the first row tried is
+ * floor(log(how_many) / log(n)), at most n - 1 (NQB_E_INVALID when it is 0, i.e.
+ * how_many < n).  Rows are tried downward while a row's pool is no smaller than the
+ * previous one, the row is at most n and the pool is within the hard limit; the answer
+ * is the row tried before the last.  NQB_E_RANGE when the first row already exceeds the
+ * limit.  If one row-0 column's pool reaches the limit the search ends there with the
+ * previous row (limit_hit = 1; the reference's own error path, n_queens.cu:176-180).
+ * Lock row 1 stands for the reference's row-1 pool, whose states hold two queens:
+ * pool_depth is then 2.
+ */
+typedef struct nqb_target {
+    unsigned lock_row;        /* the locked row the reference reports and writes           */
+    unsigned pool_depth;      /* queens per pool state: lock_row, or 2 when lock_row == 1   */
+    uint64_t count;           /* pool states                                               */
+    uint64_t hard_limit;
+    unsigned first_row;       /* rows first_row .. first_row + tried - 1 were tried          */
+    unsigned tried;
+    int limit_hit;
+    unsigned reserved;
+    uint64_t tried_count[32]; /* pool states of each tried row                             */
+} nqb_target;
+
+int nqb_pool_for_target(unsigned n, uint64_t how_many, nqb_target* target);
 
 /* Sum of the pool's weights: the number of full-board prefixes it stands for. */
 int nqb_pool_weighted_size(unsigned n, unsigned depth, uint64_t* weighted);

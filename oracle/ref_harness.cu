@@ -8,6 +8,9 @@
 //   ref_harness replay <d> [stride offset]      kernel-loop replay (GPU_NQueens.cu:338-452)
 //   ref_harness cpu    <d> <threads> [stride offset]  host DFS count (n_queens.cu:423-445)
 //   ref_harness gpu    <d> [reps]                gpu_solver_driver on the pool (GPU_NQueens.cu:56)
+//   ref_harness writemix <d1> <d2> <file>        the d1 and d2 pools interleaved state by state,
+//                                                written by util_write_nq_states_to_stream
+//   ref_harness readfile <file>                  util_read_nq_states_from_stream: count, lock, hash
 #include "deffinitions.cuh"
 #undef N
 #define N NQO_REF_N
@@ -173,6 +176,46 @@ static int cmd_gpu(unsigned d, unsigned reps) {
     return 0;
 }
 
+static int cmd_writemix(unsigned d1, unsigned d2, const char* path) {
+    uint64_t c1, c2;
+    nq_mem_handle_t *h1, *h2;
+    nq_state_t* p1 = make_pool(d1, &c1, &h1);
+    nq_state_t* p2 = make_pool(d2, &c2, &h2);
+    std::vector<nq_state_t> mix;
+    mix.reserve(c1 + c2);
+    for (uint64_t i = 0; i < c1 || i < c2; ++i) {
+        if (i < c1) mix.push_back(p1[i]);
+        if (i < c2) mix.push_back(p2[i]);
+    }
+    FILE* f = fopen(path, "wb");
+    if (!f) return 3;
+    const int w = util_write_nq_states_to_stream(f, mix.data(), mix.size(), (unsigned char)d1);
+    fclose(f);
+    printf("NQO_JSON {\"d1\": %u, \"d2\": %u, \"states\": %zu, \"hash\": \"%016" PRIx64 "\", \"status\": %d}\n", d1, d2,
+           mix.size(), pool_hash(mix.data(), mix.size()), w);
+    nq_mem_free(h1);
+    nq_mem_free(h2);
+    return w ? 4 : 0;
+}
+
+static int cmd_readfile(const char* path) {
+    FILE* f = fopen(path, "rb");
+    if (!f) return 3;
+    nq_mem_handle_t h;
+    uint64_t len = 0;
+    unsigned char lock = 0;
+    const int r = util_read_nq_states_from_stream(f, &h, &len, &lock, false);
+    fclose(f);
+    if (r) return 4;
+    const nq_state_t* p = (const nq_state_t*)h.mem_ptr;
+    uint64_t w = 0;
+    for (uint64_t i = 0; i < len; ++i) w += weight_of(&p[i]);
+    printf("NQO_JSON {\"states\": %" PRIu64 ", \"lock\": %u, \"weighted\": %" PRIu64 ", \"hash\": \"%016" PRIx64 "\"}\n",
+           len, (unsigned)lock, w, pool_hash(p, len));
+    nq_mem_free(&h);
+    return 0;
+}
+
 int main(int argc, char** argv) {
     if (argc < 3) {
         fprintf(stderr, "usage: %s pool|dump|replay|cpu|gpu <d> ...\n", argv[0]);
@@ -192,6 +235,9 @@ int main(int argc, char** argv) {
         const uint64_t offset = argc > 5 ? strtoull(argv[5], nullptr, 10) : 0;
         return cmd_cpu(d, th ? th : 1, stride ? stride : 1, offset);
     }
+    if (!strcmp(argv[1], "writemix") && argc > 4)
+        return cmd_writemix(d, (unsigned)strtoul(argv[3], nullptr, 10), argv[4]);
+    if (!strcmp(argv[1], "readfile")) return cmd_readfile(argv[2]);
     if (!strcmp(argv[1], "gpu")) return cmd_gpu(d, argc > 3 ? (unsigned)strtoul(argv[3], nullptr, 10) : 1);
     fprintf(stderr, "unknown command\n");
     return 1;

@@ -34,6 +34,17 @@ def load_nqo():
     return nqo
 
 
+def load_nqsf():
+    load_nqo()
+    import nqsf
+    return nqsf
+
+
+@pytest.fixture(scope="session")
+def nqsf():
+    return load_nqsf()
+
+
 @pytest.fixture(scope="session")
 def nqb():
     return load_nqb()
