@@ -107,6 +107,9 @@ def lib():
             "nqb_read_state_file": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_uint,
                                                    ctypes.POINTER(StateFileInfo), ctypes.POINTER(vp)]),
             "nqb_pool_for_target": (ctypes.c_int, [ctypes.c_uint, ctypes.c_uint64, ctypes.POINTER(Target)]),
+            "nqb_solve_states_multi": (ctypes.c_int, [vp, ctypes.c_uint64, vp, ctypes.c_uint, ctypes.POINTER(Opts),
+                                                      u64p, ctypes.POINTER(Stats)]),
+            "nqb_device_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -258,6 +261,24 @@ def pool_for_target(n, how_many):
     d = {k: getattr(t, k) for k, _ in Target._fields_ if k not in ("reserved", "tried_count")}
     d["tried_count"] = list(t.tried_count[:t.tried])
     return d
+
+
+def solve_states_multi(states, devices, **opts):
+    """(total, stats) of host states split in contiguous slices across `devices`."""
+    states = np.ascontiguousarray(states, dtype=STATE_DTYPE)
+    devs = (ctypes.c_int * len(devices))(*devices)
+    t = ctypes.c_uint64(0)
+    st = Stats()
+    _check(lib().nqb_solve_states_multi(states.ctypes.data, len(states), devs, len(devices),
+                                        ctypes.byref(make_opts(**opts)), ctypes.byref(t), ctypes.byref(st)),
+           "nqb_solve_states_multi")
+    return t.value, st.as_dict()
+
+
+def device_count():
+    c = ctypes.c_int(0)
+    status = lib().nqb_device_count(ctypes.byref(c))
+    return c.value if status == OK else 0
 
 
 def generate_pool_alloc(n, depth):

@@ -2,9 +2,11 @@
 // around the pool generator and the search kernels.  Replaces the reference's solve()
 // (NQ_solver.cu:192-209) and gpu_solver_driver (GPU_NQueens.cu:56-175); unlike those it
 // never exits the process and frees everything it allocated on every path.
+#include <algorithm>
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "nqb_internal.h"
@@ -209,6 +211,14 @@ const char* nqb_strerror(int s) {
 
 int nqb_version(void) { return NQB_VERSION; }
 
+int nqb_device_count(int* count) {
+    if (!count) return NQB_E_INVALID;
+    *count = 0;
+    const int s = cuda_status(cudaGetDeviceCount(count));
+    if (s) *count = 0;
+    return s ? s : (*count > 0 ? NQB_OK : NQB_E_NODEVICE);
+}
+
 int nqb_device_check(int device) {
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
@@ -311,6 +321,45 @@ int nqb_solve_states(const nqb_state* states, uint64_t count, const nqb_opts* op
     NQB_TRY(solve_host_states(sc, states, count, o, totals, nullptr, stats));
     *total = totals[0];
     if (stats) stats->wall_ms = now_ms() - t0;
+    return NQB_OK;
+}
+
+int nqb_solve_states_multi(const nqb_state* states, uint64_t count, const int* devices, unsigned ndev,
+                           const nqb_opts* opts, uint64_t* total, nqb_stats* stats) {
+    const double t0 = now_ms();
+    if (!total || (count && !states) || !devices || ndev == 0) return NQB_E_INVALID;
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    *total = 0;
+    const nqb_opts base = resolve(opts);
+    std::vector<uint64_t> part(ndev, 0);
+    std::vector<nqb_stats> pst(ndev);
+    std::vector<int> status(ndev, NQB_OK);
+    std::vector<std::thread> workers;
+    const uint64_t per = count / ndev;  // contiguous slices, the last one takes the remainder
+    for (unsigned k = 0; k < ndev; ++k) {
+        const uint64_t first = per * k, len = per + (k == ndev - 1 ? count % ndev : 0);
+        workers.emplace_back([&, k, first, len]() {
+            nqb_opts o = base;
+            o.device = devices[k];
+            status[k] = nqb_solve_states(states + first, len, &o, &part[k], &pst[k]);
+        });
+    }
+    for (auto& w : workers) w.join();
+    for (unsigned k = 0; k < ndev; ++k) NQB_TRY(status[k]);
+    for (unsigned k = 0; k < ndev; ++k) {
+        *total += part[k];
+        if (!stats) continue;
+        stats->states += pst[k].states;
+        stats->nodes += pst[k].nodes;
+        stats->h2d_ms = std::max(stats->h2d_ms, pst[k].h2d_ms);
+        stats->kernel_ms = std::max(stats->kernel_ms, pst[k].kernel_ms);
+        stats->kernel_launches += pst[k].kernel_launches;
+        stats->items += pst[k].items;
+    }
+    if (stats) {
+        stats->unit_nodes = UINT64_MAX;
+        stats->wall_ms = now_ms() - t0;
+    }
     return NQB_OK;
 }
 

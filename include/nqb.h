@@ -121,6 +121,9 @@ int nqb_version(void);
  * Replaces check_gpu_compatibility (GPU_NQueens.cu:23-54). */
 int nqb_device_check(int device);
 
+/* Number of CUDA devices visible to the process (NQB_E_NODEVICE when none). */
+int nqb_device_count(int* count);
+
 /* ---- the drop-in count -------------------------------------------------- */
 /*
  * Counts all solutions of the n-queens puzzle: builds the pool of every valid
@@ -269,6 +272,14 @@ int nqb_sample_boards(uint64_t seed, uint64_t count, unsigned n_min, unsigned n_
  */
 int nqb_solve_states(const nqb_state* states, uint64_t count, const nqb_opts* opts,
                      uint64_t* total, nqb_stats* stats);
+
+/* nqb_solve_states over several GPUs (the reference driver's configs list, GPU_NQueens.cu:
+ * 56-175): device k of `devices` gets a contiguous slice of floor(count / ndev) states, the
+ * last also the remainder (:84-90), each solved by its own host thread; the counts are
+ * summed on the host (:164-171).  Devices may repeat; opts->device is ignored.  stats: sums
+ * of states, nodes, launches and items, and the slowest device's h2d and kernel times. */
+int nqb_solve_states_multi(const nqb_state* states, uint64_t count, const int* devices, unsigned ndev,
+                           const nqb_opts* opts, uint64_t* total, nqb_stats* stats);
 
 /*
  * Per-board completion counts: out[i] = weight_i x completions of boards[i]

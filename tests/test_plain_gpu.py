@@ -163,3 +163,16 @@ def test_count_with_host_or_device_pool(nqb, form):
         c_host, s_host = nqb.count_ex(n, d, form=form, host_pool=True)
         assert c_dev == c_host == KAT[n] and s_dev["nodes"] == s_host["nodes"]
         assert s_dev["h2d_ms"] == 0.0 and s_dev["states"] == s_host["states"]
+
+
+@pytest.mark.parametrize("devices", [[0], [0, 0], [0, 0, 0]])
+def test_solve_states_multi_slices(nqb, devices):
+    pool = nqb.generate_pool(15, 5)
+    total, st = nqb.solve_states_multi(pool, devices, form=1)
+    one, st1 = nqb.solve_states_multi(pool, [0])
+    assert total == one == KAT[15] and st["nodes"] == st1["nodes"] and st["states"] == len(pool)
+    assert nqb.device_count() >= 1
+    # fewer states than devices: the first slices are empty, the last takes them all
+    t, _ = nqb.solve_states_multi(pool[:2], devices)
+    w, _ = nqb.solve_states(pool[:2])
+    assert t == w
