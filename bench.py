@@ -240,13 +240,14 @@ def run_nqb(args):
         nqb.count_ex(n, d, device=dev, form=form)  # warm-up of the call path
         if world > 1:
             dist.barrier()
-        walls, gen, h2d, ker = [], [], [], []
+        walls, gen, h2d, ker, lib_wall = [], [], [], [], []
         for _ in range(args.steps):
             t0 = time.perf_counter()
             c, st = nqb.count_ex(n, d, device=dev, form=form)
             walls.append(time.perf_counter() - t0)
             assert c == count
             gen.append(st["gen_ms"]), h2d.append(st["h2d_ms"]), ker.append(st["kernel_ms"])
+            lib_wall.append(st["wall_ms"])
         wall = max(walls) if world == 1 else None
         if world > 1:
             t = torch.tensor([max(walls)], device=f"cuda:{dev}")
@@ -258,7 +259,9 @@ def run_nqb(args):
                "h2d_bytes_per_step": 16 * ((n + 1) // 2), "d2h_bytes_per_step": 8 * d + 32,
                "wall_ms_per_step": round(1e3 * sum(walls) / len(walls), 3), "max_wall_ms": round(1e3 * wall, 3),
                "gen_ms": round(float(np.mean(gen)), 3), "h2d_ms": round(float(np.mean(h2d)), 3),
-               "kernel_ms": round(float(np.mean(ker)), 3), "api": "nqb_count_ex"}
+               "kernel_ms": round(float(np.mean(ker)), 3), "api": "nqb_count_ex",
+               "wall_ms_steps": [round(1e3 * w, 3) for w in walls],
+               "library_wall_ms_steps": [round(w, 3) for w in lib_wall]}
         t0 = time.perf_counter()
         c, st = nqb.count_ex(n, d, device=dev, form=form, host_pool=True)
         hw = time.perf_counter() - t0

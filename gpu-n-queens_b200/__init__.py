@@ -110,6 +110,7 @@ def lib():
             "nqb_solve_states_multi": (ctypes.c_int, [vp, ctypes.c_uint64, vp, ctypes.c_uint, ctypes.POINTER(Opts),
                                                       u64p, ctypes.POINTER(Stats)]),
             "nqb_device_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
+            "nqb_trim_device_memory": (ctypes.c_int, [ctypes.c_int]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -273,6 +274,11 @@ def solve_states_multi(states, devices, **opts):
                                         ctypes.byref(make_opts(**opts)), ctypes.byref(t), ctypes.byref(st)),
            "nqb_solve_states_multi")
     return t.value, st.as_dict()
+
+
+def trim_device_memory(device=0):
+    """Returns the library's cached device memory on `device` to the driver."""
+    _check(lib().nqb_trim_device_memory(device), "nqb_trim_device_memory")
 
 
 def device_count():

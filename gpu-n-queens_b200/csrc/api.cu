@@ -48,8 +48,8 @@ class Scope {
         status = cuda_status(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     }
     ~Scope() {
+        for (void* p : bufs_) dev_free(p, stream);
         if (stream) cudaStreamSynchronize(stream);
-        for (void* p : bufs_) cudaFree(p);
         for (cudaEvent_t e : events_) cudaEventDestroy(e);
         if (stream) cudaStreamDestroy(stream);
         cudaSetDevice(prev_);
@@ -57,7 +57,7 @@ class Scope {
     template <class T>
     int alloc(T** p, size_t bytes) {
         void* v = nullptr;
-        const int s = cuda_status(cudaMalloc(&v, bytes ? bytes : 16));
+        const int s = dev_alloc_bytes(&v, bytes, stream);
         if (s != NQB_OK) return s;
         bufs_.push_back(v);
         *p = static_cast<T*>(v);
@@ -152,12 +152,15 @@ int solve_device_states(Scope& sc, const nqb_state* d_states, uint64_t count, un
 
 // Solves `count` host states on the device with the form o.form; fills totals
 // {count, nodes, unit, err} and, if per_state != nullptr, per-state weighted counts.
+// `known_depth` != 0: the states come from the library's own generator, so the
+// per-state validation and the stack-depth scan are skipped.
 int solve_host_states(Scope& sc, const nqb_state* states, uint64_t count, const nqb_opts& o,
                       unsigned long long totals[4], uint64_t* per_state, nqb_stats* st,
-                      uint64_t* per_state_nodes = nullptr) {
-    for (uint64_t i = 0; i < count; ++i)
-        if (!state_valid(states[i])) return NQB_E_INVALID;
-    const unsigned depth = max_stack_depth(states, count);
+                      uint64_t* per_state_nodes = nullptr, unsigned known_depth = 0) {
+    if (!known_depth)
+        for (uint64_t i = 0; i < count; ++i)
+            if (!state_valid(states[i])) return NQB_E_INVALID;
+    const unsigned depth = known_depth ? known_depth : max_stack_depth(states, count);
     nqb_state* d_states = nullptr;
     NQB_TRY(sc.alloc(&d_states, count * sizeof(nqb_state)));
     cudaEvent_t e0;
@@ -226,9 +229,12 @@ int nqb_device_check(int device) {
         return NQB_E_NODEVICE;
     }
     if (device < 0 || device >= n) return NQB_E_NODEVICE;
-    cudaDeviceProp p;
-    if (cudaGetDeviceProperties(&p, device) != cudaSuccess) return NQB_E_NODEVICE;
-    if (p.major != 10 || p.warpSize != 32 || p.computeMode == cudaComputeModeProhibited) return NQB_E_NODEVICE;
+    int major = 0, warp = 0, mode = 0;  // single attributes: cheaper than the whole cudaDeviceProp
+    if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&warp, cudaDevAttrWarpSize, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&mode, cudaDevAttrComputeMode, device) != cudaSuccess)
+        return NQB_E_NODEVICE;
+    if (major != 10 || warp != 32 || mode == cudaComputeModeProhibited) return NQB_E_NODEVICE;
     return NQB_OK;
 }
 
@@ -276,7 +282,8 @@ int nqb_count_ex(unsigned n, unsigned depth, const nqb_opts* opts, uint64_t* cou
         const double tg = now_ms();
         NQB_TRY(nqb_generate_pool(n, depth, &pool, &cnt));
         gen_ms = now_ms() - tg;
-        const int s = solve_host_states(sc, pool, cnt, o, totals, nullptr, stats);
+        const int s = solve_host_states(sc, pool, cnt, o, totals, nullptr, stats, nullptr,
+                                        n - depth - 1 > 0 ? n - depth - 1 : 1);
         std::free(pool);
         NQB_TRY(s);
     } else {  // build the pool on the GPU: nothing crosses PCIe but the result
@@ -290,7 +297,7 @@ int nqb_count_ex(unsigned n, unsigned depth, const nqb_opts* opts, uint64_t* cou
         cudaEventRecord(g1, sc.stream);
         const int s = solve_device_states(sc, d_pool, cnt, n - depth - 1 > 0 ? n - depth - 1 : 1, o, totals, nullptr,
                                           stats, nullptr, nullptr);
-        cudaFreeAsync(d_pool, sc.stream);
+        dev_free(d_pool, sc.stream);
         NQB_TRY(s);
         float g = 0.0f;
         cudaEventElapsedTime(&g, g0, g1);
@@ -467,12 +474,12 @@ int nqb_generate_pool_device_into(unsigned n, unsigned depth, nqb_state* d_buf, 
     if (s) return s;
     if (*count > capacity) s = NQB_E_RANGE;
     else if (*count) s = cuda_status(cudaMemcpyAsync(d_buf, d_pool, *count * sizeof(nqb_state), cudaMemcpyDeviceToDevice, st));
-    cudaFreeAsync(d_pool, st);
+    dev_free(d_pool, st);
     return s;
 }
 
 void nqb_free_device(void* p, void* stream) {
-    if (p) cudaFreeAsync(p, static_cast<cudaStream_t>(stream));
+    dev_free(p, static_cast<cudaStream_t>(stream));
 }
 
 }  // extern "C"

@@ -87,6 +87,19 @@ int launch_batched_scheduled(const nqb_state* d_items, uint32_t n, const uint32_
                              unsigned long long* d_per_board_nodes, const nqb_opts& o, unsigned stack_depth,
                              int device, cudaStream_t s, unsigned* launches, SchedInfo* info);
 
+// Stream-ordered device allocation from the library's pool on the current device
+// (devmem.cu); release with dev_free on a stream.  Freed memory stays cached for later
+// calls until nqb_trim_device_memory.
+int dev_alloc_bytes(void** p, size_t bytes, cudaStream_t s);
+template <class T>
+int dev_alloc(T** p, size_t bytes, cudaStream_t s) {
+    void* v = nullptr;
+    const int st = dev_alloc_bytes(&v, bytes, s);
+    *p = static_cast<T*>(v);
+    return st;
+}
+void dev_free(void* p, cudaStream_t s);
+
 int cuda_status(cudaError_t e);
 
 // Learned cost model (mlp.cu): predicted log2(1 + nodes) of `count` device states.

@@ -57,12 +57,12 @@ int scan_total(const uint32_t* k, uint32_t* offs, uint32_t m, cudaStream_t s, ui
     size_t tb = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, tb, k, offs, m, s);
     void* tmp = nullptr;
-    int st = cuda_status(cudaMallocAsync(&tmp, tb ? tb : 1, s));
+    int st = dev_alloc_bytes(&tmp, tb, s);
     if (!st) st = cuda_status(cub::DeviceScan::ExclusiveSum(tmp, tb, k, offs, m, s));
     uint32_t last_k = 0, last_o = 0;
     if (!st) st = cuda_status(cudaMemcpyAsync(&last_k, k + (m - 1), 4, cudaMemcpyDeviceToHost, s));
     if (!st) st = cuda_status(cudaMemcpyAsync(&last_o, offs + (m - 1), 4, cudaMemcpyDeviceToHost, s));
-    if (tmp) cudaFreeAsync(tmp, s);
+    if (tmp) dev_free(tmp, s);
     if (!st) st = cuda_status(cudaStreamSynchronize(s));
     *total = (uint64_t)last_o + last_k;
     return st;
@@ -83,13 +83,13 @@ int generate_pool_device(unsigned n, unsigned depth, cudaStream_t s, nqb_state**
     }
     uint4* cur = nullptr;
     uint64_t m = seed.size();
-    int st = cuda_status(cudaMallocAsync(reinterpret_cast<void**>(&cur), m * sizeof(uint4), s));
+    int st = dev_alloc(&cur, m * sizeof(uint4), s);
     if (!st) st = cuda_status(cudaMemcpyAsync(cur, seed.data(), m * sizeof(uint4), cudaMemcpyHostToDevice, s));
     uint32_t *k = nullptr, *offs = nullptr;
     for (unsigned row = 1; !st; ++row) {
         const bool last = row == depth;
-        if ((st = cuda_status(cudaMallocAsync(reinterpret_cast<void**>(&k), m * sizeof(uint32_t), s)))) break;
-        if ((st = cuda_status(cudaMallocAsync(reinterpret_cast<void**>(&offs), m * sizeof(uint32_t), s)))) break;
+        if ((st = dev_alloc(&k, m * sizeof(uint32_t), s))) break;
+        if ((st = dev_alloc(&offs, m * sizeof(uint32_t), s))) break;
         const unsigned grid = (unsigned)((m + 255) / 256);
         child_count_kernel<<<grid, 256, 0, s>>>(cur, (uint32_t)m, last ? 1 : 0, k);
         uint64_t total = 0;
@@ -99,17 +99,17 @@ int generate_pool_device(unsigned n, unsigned depth, cudaStream_t s, nqb_state**
             break;
         }
         uint4* next = nullptr;
-        if ((st = cuda_status(cudaMallocAsync(reinterpret_cast<void**>(&next), (total ? total : 1) * sizeof(uint4), s))))
+        if ((st = dev_alloc(&next, total * sizeof(uint4), s)))
             break;
         if (last) keep_kernel<<<grid, 256, 0, s>>>(cur, (uint32_t)m, k, offs, next);
         else expand_kernel<<<grid, 256, 0, s>>>(cur, (uint32_t)m, offs, next);
         if ((st = cuda_status(cudaGetLastError()))) {
-            cudaFreeAsync(next, s);
+            dev_free(next, s);
             break;
         }
-        cudaFreeAsync(cur, s);
-        cudaFreeAsync(k, s);
-        cudaFreeAsync(offs, s);
+        dev_free(cur, s);
+        dev_free(k, s);
+        dev_free(offs, s);
         k = offs = nullptr;
         cur = next;
         m = total;
@@ -119,10 +119,10 @@ int generate_pool_device(unsigned n, unsigned depth, cudaStream_t s, nqb_state**
             break;
         }
     }
-    if (k) cudaFreeAsync(k, s);
-    if (offs) cudaFreeAsync(offs, s);
+    if (k) dev_free(k, s);
+    if (offs) dev_free(offs, s);
     if (st) {
-        if (cur) cudaFreeAsync(cur, s);
+        if (cur) dev_free(cur, s);
         return st;
     }
     *d_out = reinterpret_cast<nqb_state*>(cur);

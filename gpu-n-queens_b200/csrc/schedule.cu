@@ -25,7 +25,7 @@
 namespace nqb {
 namespace {
 
-// Stream-ordered device buffer (cudaMallocAsync from the device's default pool): no
+// Stream-ordered device buffer (from the library's device memory pool): no
 // device-wide synchronisation on allocation or release, and pool memory is reused across
 // calls.
 template <class T>
@@ -35,10 +35,10 @@ struct Buf {
     cudaStream_t s = nullptr;
     explicit Buf(cudaStream_t st) : s(st) {}
     int alloc(size_t count) {
-        if (p) cudaFreeAsync(p, s);
+        if (p) dev_free(p, s);
         p = nullptr;
         n = count;
-        return cuda_status(cudaMallocAsync(reinterpret_cast<void**>(&p), (count ? count : 1) * sizeof(T), s));
+        return dev_alloc(&p, count * sizeof(T), s);
     }
     T* take() {
         T* q = p;
@@ -46,7 +46,7 @@ struct Buf {
         return q;
     }
     ~Buf() {
-        if (p) cudaFreeAsync(p, s);
+        if (p) dev_free(p, s);
     }
 };
 
@@ -217,9 +217,9 @@ int schedule_items(const nqb_state* d_items, uint32_t n, const uint32_t* d_board
 }
 
 void Schedule::release() {
-    if (owned_items) cudaFreeAsync(owned_items, stream);
-    if (owned_board) cudaFreeAsync(owned_board, stream);
-    if (owned_order) cudaFreeAsync(owned_order, stream);
+    if (owned_items) dev_free(owned_items, stream);
+    if (owned_board) dev_free(owned_board, stream);
+    if (owned_order) dev_free(owned_order, stream);
     owned_items = nullptr;
     owned_board = nullptr;
     owned_order = nullptr;

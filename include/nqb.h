@@ -121,6 +121,11 @@ int nqb_version(void);
  * Replaces check_gpu_compatibility (GPU_NQueens.cu:23-54). */
 int nqb_device_check(int device);
 
+/* Device buffers of a call (the pool, its level buffers, scratch) come from the library's
+ * own stream-ordered memory pool on that device and stay cached for the next call instead
+ * of being unmapped; this returns the cached memory of `device` to the driver. */
+int nqb_trim_device_memory(int device);
+
 /* Number of CUDA devices visible to the process (NQB_E_NODEVICE when none). */
 int nqb_device_count(int* count);
 

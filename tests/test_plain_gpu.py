@@ -176,3 +176,15 @@ def test_solve_states_multi_slices(nqb, devices):
     t, _ = nqb.solve_states_multi(pool[:2], devices)
     w, _ = nqb.solve_states(pool[:2])
     assert t == w
+
+
+def test_cached_device_memory_reused_and_trimmed(nqb):
+    """Repeated calls reuse the library's cached device memory; trimming returns it and
+    the next call maps it again, with the same result."""
+    for _ in range(3):
+        assert nqb.count(16, 5, form=1) == KAT[16]
+    nqb.trim_device_memory(0)
+    assert nqb.count(16, 5) == KAT[16]
+    nqb.trim_device_memory(0)
+    with pytest.raises(nqb.NQBError):
+        nqb.trim_device_memory(-1)
