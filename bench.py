@@ -51,6 +51,25 @@ def rank_env():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
+def max_over_ranks(x, world, device=None):
+    """The maximum of a per-rank time over all ranks (an all-reduce MAX of one value): a
+    CUDA tensor on `device` under NCCL, a CPU tensor under gloo; `x` itself at world 1."""
+    if world == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    dev = "cpu" if dist.get_backend() == "gloo" else device
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(units_per_rank, world, seconds_max):
+    """Whole-job throughput of `world` independent replicas: every rank processes the same
+    units, and the job takes as long as its slowest rank."""
+    return units_per_rank * world / seconds_max
+
+
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -209,12 +228,9 @@ def run_nqb(args):
     ms = ev0.elapsed_time(ev1)
     res = d_out.cpu().numpy().astype(np.uint64)
     assert all(int(res[i, 0]) == count and int(res[i, 1]) == nodes for i in range(args.steps))
-    if world > 1:
-        t = torch.tensor([ms], device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, world, f"cuda:{dev}")
     ms_step = ms / args.steps
-    value = nodes * world / (ms_step / 1e3)
+    value = replica_rate(nodes, world, ms_step / 1e3)
 
     # the other form once on the same resident pool, for the plain-vs-batched comparison
     forms = {args.form: {"ms": round(ms_step, 3), "nodes_per_s": round(nodes / (ms_step / 1e3), 1)}}
@@ -248,16 +264,13 @@ def run_nqb(args):
             assert c == count
             gen.append(st["gen_ms"]), h2d.append(st["h2d_ms"]), ker.append(st["kernel_ms"])
             lib_wall.append(st["wall_ms"])
-        wall = max(walls) if world == 1 else None
-        if world > 1:
-            t = torch.tensor([max(walls)], device=f"cuda:{dev}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            wall = float(t.item())
+        wall = max_over_ranks(max(walls), world, f"cuda:{dev}")
+        mean_wall = max_over_ranks(sum(walls) / len(walls), world, f"cuda:{dev}")
         # host->device: the row-0 seed states; device->host: 8 bytes of scan totals per pool
         # level, then the 32-byte result
-        e2e = {"value": nodes * world / (sum(walls) / len(walls)), "unit": "nodes/s",
+        e2e = {"value": replica_rate(nodes, world, mean_wall), "unit": "nodes/s",
                "h2d_bytes_per_step": 16 * ((n + 1) // 2), "d2h_bytes_per_step": 8 * d + 32,
-               "wall_ms_per_step": round(1e3 * sum(walls) / len(walls), 3), "max_wall_ms": round(1e3 * wall, 3),
+               "wall_ms_per_step": round(1e3 * mean_wall, 3), "max_wall_ms": round(1e3 * wall, 3),
                "gen_ms": round(float(np.mean(gen)), 3), "h2d_ms": round(float(np.mean(h2d)), 3),
                "kernel_ms": round(float(np.mean(ker)), 3), "api": "nqb_count_ex",
                "wall_ms_steps": [round(1e3 * w, 3) for w in walls],
