@@ -111,6 +111,8 @@ def lib():
                                                       u64p, ctypes.POINTER(Stats)]),
             "nqb_device_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
             "nqb_trim_device_memory": (ctypes.c_int, [ctypes.c_int]),
+            "nqb_measure_int32_peak": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                                      ctypes.POINTER(ctypes.c_double)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -274,6 +276,14 @@ def solve_states_multi(states, devices, **opts):
                                         ctypes.byref(make_opts(**opts)), ctypes.byref(t), ctypes.byref(st)),
            "nqb_solve_states_multi")
     return t.value, st.as_dict()
+
+
+def measure_int32_peak(device=0):
+    """(best, {kind: lane-ops/s}) of the INT32 issue-rate microbenchmark."""
+    best = ctypes.c_double(0)
+    kinds = (ctypes.c_double * 4)()
+    _check(lib().nqb_measure_int32_peak(device, ctypes.byref(best), kinds), "nqb_measure_int32_peak")
+    return best.value, dict(zip(("lop3", "add", "imad", "lop3_imad"), list(kinds)))
 
 
 def trim_device_memory(device=0):

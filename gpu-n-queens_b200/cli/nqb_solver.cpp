@@ -15,7 +15,6 @@
 // option, -n/--board (default 17), or taken from the file with -l.  -f/--form picks the
 // search form (batched by default, or plain).
 #include <cerrno>
-#include <chrono>
 #include <cinttypes>
 #include <climits>
 #include <cmath>

@@ -343,13 +343,18 @@ int nqb_solve_states_multi(const nqb_state* states, uint64_t count, const int* d
     std::vector<int> status(ndev, NQB_OK);
     std::vector<std::thread> workers;
     const uint64_t per = count / ndev;  // contiguous slices, the last one takes the remainder
-    for (unsigned k = 0; k < ndev; ++k) {
+    auto work = [&](unsigned k) {
         const uint64_t first = per * k, len = per + (k == ndev - 1 ? count % ndev : 0);
-        workers.emplace_back([&, k, first, len]() {
-            nqb_opts o = base;
-            o.device = devices[k];
-            status[k] = nqb_solve_states(states + first, len, &o, &part[k], &pst[k]);
-        });
+        nqb_opts o = base;
+        o.device = devices[k];
+        status[k] = nqb_solve_states(states + first, len, &o, &part[k], &pst[k]);
+    };
+    for (unsigned k = 0; k < ndev; ++k) {
+        try {  // no exception may cross the C ABI: without a thread, solve the slice here
+            workers.emplace_back(work, k);
+        } catch (...) {
+            work(k);
+        }
     }
     for (auto& w : workers) w.join();
     for (unsigned k = 0; k < ndev; ++k) NQB_TRY(status[k]);

@@ -138,8 +138,12 @@ int generate_pool_ex(unsigned n, unsigned depth, nqb_state* buf, nqb_placement* 
             return;
         }
         std::vector<std::thread> ts;
-        ts.reserve(nt);
-        for (unsigned i = 0; i < nt; ++i) ts.emplace_back(body);
+        try {  // tasks are claimed from a shared counter, so fewer threads only take longer
+            ts.reserve(nt);
+            for (unsigned i = 0; i < nt; ++i) ts.emplace_back(body);
+        } catch (...) {
+        }
+        body();
         for (auto& t : ts) t.join();
     };
     parallel([&](size_t k) { sizes[k] = run_task(tasks[k], nullptr, nullptr); });

@@ -126,6 +126,12 @@ int nqb_device_check(int device);
  * of being unmapped; this returns the cached memory of `device` to the driver. */
 int nqb_trim_device_memory(int device);
 
+/* Measures the integer lane-ops per second `device` sustains (the search kernels'
+ * roofline denominator): every SM at full occupancy running independent chains of one
+ * integer instruction kind.  per_kind (optional, 4 entries): LOP3, add, IMAD, and LOP3 and
+ * IMAD alternated; *best = the largest.  Takes about 0.1 s. */
+int nqb_measure_int32_peak(int device, double* best, double* per_kind);
+
 /* Number of CUDA devices visible to the process (NQB_E_NODEVICE when none). */
 int nqb_device_count(int* count);
 

@@ -188,3 +188,11 @@ def test_cached_device_memory_reused_and_trimmed(nqb):
     nqb.trim_device_memory(0)
     with pytest.raises(nqb.NQBError):
         nqb.trim_device_memory(-1)
+
+
+def test_int32_peak_microbenchmark(nqb):
+    """The roofline denominator: every kind runs, and the best is within the issue limit
+    (one warp instruction per SM sub-partition per clock at the maximum SM clock)."""
+    best, kinds = nqb.measure_int32_peak(0)
+    assert set(kinds) == {"lop3", "add", "imad", "lop3_imad"} and all(v > 1e12 for v in kinds.values())
+    assert best == max(kinds.values()) and best <= 148 * 4 * 32 * 2.0e9 * 1.02
