@@ -198,13 +198,22 @@ def run_nqb(args):
     sptr = stream.cuda_stream
     form = {"plain": nqb.FORM_PLAIN, "batched": nqb.FORM_BATCHED}[args.form]
 
+    # autotuned launch: every form and block size timed on a 1/64 stride sample of the pool
+    # (depths d-1..d+1 are tuned too: the pick over all of them is run as a full count in extras)
+    tuning, blocks = None, {nqb.FORM_PLAIN: args.block, nqb.FORM_BATCHED: args.block}
+    if not args.block and not args.no_tune:
+        tuning = nqb.tune_count(n, [x for x in (d - 1, d, d + 1) if 1 <= x < n], sample_div=64, device=dev)
+        for f in blocks:
+            blocks[f] = min((t for t in tuning["tried"] if t["form"] == f and t["depth"] == d),
+                            key=lambda t: t["ms"])["block_size"]
+
     def launch(f, out_row, head_slot):
         if f == nqb.FORM_PLAIN:
-            nqb.plain_launch(d_pool.data_ptr(), states, out_row.data_ptr(), block_size=args.block,
+            nqb.plain_launch(d_pool.data_ptr(), states, out_row.data_ptr(), block_size=blocks[f],
                              stack_depth=stack_depth, stream=sptr)
         else:
             nqb.batched_launch(d_pool.data_ptr(), states, head_slot.data_ptr(), out_row.data_ptr(),
-                               block_size=args.block, stack_depth=stack_depth, stream=sptr)
+                               block_size=blocks[f], stack_depth=stack_depth, stream=sptr)
 
     def step(i):
         launch(form, d_out[i], d_head[i:i + 1])
@@ -265,13 +274,13 @@ def run_nqb(args):
     # e2e: the public C ABI call with host buffers, every step
     e2e = None
     if not args.skip_e2e:
-        nqb.count_ex(n, d, device=dev, form=form)  # warm-up of the call path
+        nqb.count_ex(n, d, device=dev, form=form, block_size=blocks[form])  # warm-up of the call path
         if world > 1:
             dist.barrier()
         walls, gen, h2d, ker, lib_wall = [], [], [], [], []
         for _ in range(args.steps):
             t0 = time.perf_counter()
-            c, st = nqb.count_ex(n, d, device=dev, form=form)
+            c, st = nqb.count_ex(n, d, device=dev, form=form, block_size=blocks[form])
             walls.append(time.perf_counter() - t0)
             assert c == count
             gen.append(st["gen_ms"]), h2d.append(st["h2d_ms"]), ker.append(st["kernel_ms"])
@@ -288,7 +297,7 @@ def run_nqb(args):
                "wall_ms_steps": [round(1e3 * w, 3) for w in walls],
                "library_wall_ms_steps": [round(w, 3) for w in lib_wall]}
         t0 = time.perf_counter()
-        c, st = nqb.count_ex(n, d, device=dev, form=form, host_pool=True)
+        c, st = nqb.count_ex(n, d, device=dev, form=form, block_size=blocks[form], host_pool=True)
         hw = time.perf_counter() - t0
         assert c == count
         e2e["host_pool"] = {"wall_ms": round(1e3 * hw, 3), "gen_ms": round(st["gen_ms"], 3),
@@ -298,6 +307,14 @@ def run_nqb(args):
     extras = None
     if rank == 0 and world == 1 and not args.skip_extras:
         extras = run_extras(nqb, dev, args)
+        if tuning:  # the autotuner's own pick (depth, form, block) as a full count
+            t0 = time.perf_counter()
+            c, st = nqb.count_ex(n, tuning["depth"], device=dev, form=tuning["form"], block_size=tuning["block_size"])
+            wall = time.perf_counter() - t0
+            extras["autotuned_count"] = {
+                "picked": {k: tuning[k] for k in ("depth", "form", "block_size", "split_factor")},
+                "count": c, "count_ok": c == count, "wall_ms": round(1e3 * wall, 3), "kernel_ms": round(st["kernel_ms"], 3),
+                "over_headline_e2e": round(e2e["wall_ms_per_step"] / (1e3 * wall), 3) if e2e else None}
 
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
@@ -320,7 +337,8 @@ def run_nqb(args):
             "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic (the full depth-7 pool of the N=21 board)",
             "config": {"workload": f"full count N={n}, pregen depth {d}", "n": n, "depth": d, "form": args.form,
-                       "states": states, "nodes": nodes, "count": count, "block": args.block or 128,
+                       "states": states, "nodes": nodes, "count": count, "block": blocks[form] or 128,
+                       "other_form_block": blocks[1 - form] or 128, "tuning": tuning,
                        "parallelism": f"replicas{world}" if world > 1 else "single",
                        "l2": f"inputs larger than L2 (pool {states * 16 / 1e6:.0f} MB)"},
             "forms": forms,
@@ -471,6 +489,7 @@ def main():
     ap.add_argument("--ref-cuda-d", type=int, default=7)
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="skip the launch autotuner (default block sizes)")
     args = ap.parse_args()
     if args.warmup < 1:
         args.warmup = 1

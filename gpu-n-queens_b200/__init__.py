@@ -40,7 +40,7 @@ class Opts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("form", ctypes.c_int), ("block_size", ctypes.c_int),
                 ("count_unit_nodes", ctypes.c_int), ("max_split_rounds", ctypes.c_int),
                 ("split_factor", ctypes.c_int), ("model", ctypes.c_void_p), ("host_pool", ctypes.c_int),
-                ("reserved", ctypes.c_int * 7)]
+                ("autotune", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
 
 
 class Stats(ctypes.Structure):
@@ -48,7 +48,7 @@ class Stats(ctypes.Structure):
                 ("gen_ms", ctypes.c_double), ("h2d_ms", ctypes.c_double), ("kernel_ms", ctypes.c_double),
                 ("wall_ms", ctypes.c_double), ("pregen_depth", ctypes.c_uint32),
                 ("kernel_launches", ctypes.c_uint32), ("items", ctypes.c_uint64), ("sched_ms", ctypes.c_double),
-                ("reserved", ctypes.c_uint32 * 2)]
+                ("block_size", ctypes.c_uint32), ("form", ctypes.c_int32)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
@@ -107,6 +107,8 @@ def lib():
             "nqb_read_state_file": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_uint,
                                                    ctypes.POINTER(StateFileInfo), ctypes.POINTER(vp)]),
             "nqb_pool_for_target": (ctypes.c_int, [ctypes.c_uint, ctypes.c_uint64, ctypes.POINTER(Target)]),
+            "nqb_tune_count": (ctypes.c_int, [ctypes.c_uint, vp, ctypes.c_uint, ctypes.POINTER(Opts), ctypes.c_uint,
+                                              ctypes.POINTER(TuneResult)]),
             "nqb_solve_states_multi": (ctypes.c_int, [vp, ctypes.c_uint64, vp, ctypes.c_uint, ctypes.POINTER(Opts),
                                                       u64p, ctypes.POINTER(Stats)]),
             "nqb_device_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
@@ -135,13 +137,14 @@ def _check(status, what):
 
 
 def make_opts(device=0, form=FORM_PLAIN, block_size=0, count_unit_nodes=False, model=None, max_split_rounds=-1,
-              split_factor=0, host_pool=False):
+              split_factor=0, host_pool=False, autotune=False):
     o = Opts()
     lib().nqb_default_opts(ctypes.byref(o))
     o.device, o.form, o.block_size = device, form, block_size
     o.count_unit_nodes, o.max_split_rounds, o.split_factor = int(count_unit_nodes), max_split_rounds, split_factor
     o.model = model.handle if model is not None else None
     o.host_pool = int(host_pool)
+    o.autotune = int(autotune)
     return o
 
 
@@ -248,6 +251,32 @@ def read_state_file(path, header=True, expect_n=0):
            f"nqb_read_state_file({path})")
     pl = np.frombuffer(_take(p, 32 * info.count), dtype=PLACEMENT_DTYPE).copy()
     return {k: getattr(info, k) for k, _ in StateFileInfo._fields_}, pl
+
+
+class TuneEntry(ctypes.Structure):
+    _fields_ = [("depth", ctypes.c_uint), ("form", ctypes.c_int), ("block_size", ctypes.c_int),
+                ("split_factor", ctypes.c_int), ("ms", ctypes.c_double)]
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [("depth", ctypes.c_uint), ("form", ctypes.c_int), ("block_size", ctypes.c_int),
+                ("split_factor", ctypes.c_int), ("best_ms", ctypes.c_double), ("sample_states", ctypes.c_uint64),
+                ("sample_div", ctypes.c_uint), ("n_tried", ctypes.c_uint), ("tried", TuneEntry * 64)]
+
+
+def tune_count(n, depths, sample_div=64, **opts):
+    """Launch autotuner (nqb_tune_count): the fastest (depth, form, block size, split factor)
+    on a 1/sample_div stride sample of each depth's pool, with every candidate's time."""
+    if isinstance(depths, int):
+        depths = [depths]
+    ds = (ctypes.c_uint * len(depths))(*depths)
+    r = TuneResult()
+    _check(lib().nqb_tune_count(n, ds, len(depths), ctypes.byref(make_opts(**opts)), sample_div, ctypes.byref(r)),
+           f"nqb_tune_count({n}, {list(depths)})")
+    keys = ("depth", "form", "block_size", "split_factor")
+    return {**{k: getattr(r, k) for k in keys}, "best_ms": r.best_ms, "sample_states": r.sample_states,
+            "sample_div": r.sample_div,
+            "tried": [{**{k: getattr(e, k) for k in keys}, "ms": round(e.ms, 3)} for e in r.tried[:r.n_tried]]}
 
 
 class Target(ctypes.Structure):

@@ -146,6 +146,8 @@ int solve_device_states(Scope& sc, const nqb_state* d_states, uint64_t count, un
         st->kernel_launches = launches;
         st->items = sched.items;
         st->sched_ms = sched.sched_ms;
+        st->block_size = (uint32_t)(o.block_size ? o.block_size : 128);
+        st->form = o.form;
     }
     return NQB_OK;
 }
@@ -270,7 +272,14 @@ int nqb_generate_pool(unsigned n, unsigned depth, nqb_state** states, uint64_t* 
 int nqb_count_ex(unsigned n, unsigned depth, const nqb_opts* opts, uint64_t* count, nqb_stats* stats) {
     const double t0 = now_ms();
     if (!count || n < NQB_MIN_N || n > NQB_MAX_N || depth < 1 || depth >= n) return NQB_E_INVALID;
-    const nqb_opts o = resolve(opts);
+    nqb_opts o = resolve(opts);
+    if (o.autotune) {  // pick the launch on a sample of this pool first
+        nqb_tune_result t;
+        NQB_TRY(nqb_tune_count(n, &depth, 1, &o, 64, &t));
+        o.form = t.form;
+        o.block_size = t.block_size;
+        o.split_factor = t.split_factor;
+    }
     if (stats) std::memset(stats, 0, sizeof(*stats));
     Scope sc(o.device);
     NQB_TRY(sc.status);

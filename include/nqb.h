@@ -91,7 +91,9 @@ typedef struct nqb_opts {
                              NULL = FIFO: items in the given order, no splitting        */
     int host_pool;        /* nqb_count_ex: 1 = build the pool on the host and copy it to
                              the GPU (the reference's way); 0 = build it on the GPU    */
-    int reserved[7];
+    int autotune;         /* nqb_count_ex: 1 = pick form, block size and split factor with
+                             nqb_tune_count on a 1/64 sample of the pool first          */
+    int reserved[6];
 } nqb_opts;
 
 typedef struct nqb_stats {
@@ -106,7 +108,8 @@ typedef struct nqb_stats {
     uint32_t kernel_launches;
     uint64_t items;      /* items the search kernel was given (after learned splitting) */
     double sched_ms;     /* learned scheduling: prediction, splitting, ordering        */
-    uint32_t reserved[2];
+    uint32_t block_size; /* threads per block of the search launch                        */
+    int32_t form;        /* search form used (NQB_FORM_*)                                  */
 } nqb_stats;
 
 /* Fills `opts` with the defaults (device 0, plain form, library block size). */
@@ -257,6 +260,38 @@ typedef struct nqb_target {
 } nqb_target;
 
 int nqb_pool_for_target(unsigned n, uint64_t how_many, nqb_target* target);
+
+/* ---- launch autotuner ------------------------------------------------------------ */
+/*
+ * Picks the launch of a full count by timing: for each depth in `depths` the pool is built
+ * on the GPU and every `sample_div`-th state taken (an unbiased 1/sample_div sample of the
+ * count's work, in pool order); on it every candidate runs twice and the faster time
+ * counts.  Candidates: both forms x block sizes 64, 128, 256, and with opts->model the
+ * batched form's split factors 1, 4, 16.  All candidates of a depth must agree on the
+ * sample's count (else NQB_E_DEVICE).  The fastest is reported with every candidate tried.
+ */
+typedef struct nqb_tune_entry {
+    unsigned depth;
+    int form;
+    int block_size;
+    int split_factor;
+    double ms;
+} nqb_tune_entry;
+
+typedef struct nqb_tune_result {
+    unsigned depth;          /* the fastest candidate                                  */
+    int form;
+    int block_size;
+    int split_factor;
+    double best_ms;          /* its time on the sample                                  */
+    uint64_t sample_states;  /* states in its depth's sample                            */
+    unsigned sample_div;
+    unsigned n_tried;
+    nqb_tune_entry tried[64];
+} nqb_tune_result;
+
+int nqb_tune_count(unsigned n, const unsigned* depths, unsigned n_depths, const nqb_opts* opts,
+                   unsigned sample_div, nqb_tune_result* out);
 
 /* Sum of the pool's weights: the number of full-board prefixes it stands for. */
 int nqb_pool_weighted_size(unsigned n, unsigned depth, uint64_t* weighted);

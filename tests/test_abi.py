@@ -1,6 +1,7 @@
 """The C ABI: libnqb.so loads, exports every function include/nqb.h declares, and rejects bad
 arguments with status codes (never exiting).  No GPU needed: no compute call is made."""
 import ctypes
+import os
 import subprocess
 
 import pytest
@@ -56,3 +57,32 @@ def test_default_opts(nqb):
     o = nqb.make_opts()
     assert (o.device, o.form, o.block_size, o.count_unit_nodes, o.max_split_rounds, o.split_factor) == (0, 0, 0, 0, -1, 0)
     assert not o.model
+
+
+def test_struct_layouts_match_header(nqb, tmp_path):
+    """Every ctypes structure of the binding has the header's size and field offsets (a C
+    program compiled against include/nqb.h prints them)."""
+    from conftest import ROOT
+    structs = {"nqb_opts": nqb.Opts, "nqb_stats": nqb.Stats, "nqb_state_file": nqb.StateFileInfo,
+               "nqb_target": nqb.Target, "nqb_tune_entry": nqb.TuneEntry, "nqb_tune_result": nqb.TuneResult}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "nqb.h"', "int main(void) {"]
+    for cname, cls in structs.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f in cls._fields_:
+            lines.append(f'printf("{cname} {f[0]} %zu\\n", offsetof({cname}, {f[0]}));')
+    lines += ['printf("nqb_placement size %zu\\n", sizeof(nqb_placement));',
+              'printf("nqb_state size %zu\\n", sizeof(nqb_state));', "return 0; }"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines():
+        name, field, val = line.split()
+        got[(name, field)] = int(val)
+    for cname, cls in structs.items():
+        assert got[(cname, "size")] == ctypes.sizeof(cls), cname
+        for f in cls._fields_:
+            assert got[(cname, f[0])] == getattr(cls, f[0]).offset, (cname, f[0])
+    assert got[("nqb_placement", "size")] == nqb.PLACEMENT_DTYPE.itemsize == 32
+    assert got[("nqb_state", "size")] == nqb.STATE_DTYPE.itemsize == 16
