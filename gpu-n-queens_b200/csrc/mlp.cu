@@ -1,8 +1,9 @@
 // Learned cost model: an MLP 112 -> 128 -> 128 -> 1 (GELU) that predicts log2 of the number
 // of search nodes below a state.  Trained on the GPU by the kernels in this file (FP16
-// operands, FP32 accumulation on the tensor cores through mma.sync m16n8k16; FP32 master
-// weights, Adam), on node counts the batched search kernel records per item.  Used only to
-// order and split the batched form's queue (schedule.cu); counts never depend on it.
+// operands, FP32 accumulation on the tensor cores; FP32 master weights, Adam), on node
+// counts the batched search kernel records per item; inference (predict_kernel) runs on
+// tcgen05 with the accumulator in tensor memory.  Used only to order and split the batched
+// form's queue (schedule.cu); counts never depend on it.
 //
 // Training step on a batch of B rows (X: B x 112 fp16):
 //   Z1 = X W1           H1 = gelu(Z1 + b1)      (fp16 copy of H1 feeds the next GEMM)
@@ -210,102 +211,213 @@ __global__ void to_half_kernel(const float* __restrict__ p, __half* __restrict__
     if (i < kH * kH) w2h[i] = __float2half(p[kW2 + i]);
 }
 
-// ---- fused inference: features -> layer 1 -> layer 2 -> head, 64 states per tile ------
-// Weights stay in shared memory for the whole (persistent) block: W1 and W2 transposed to
-// [out][in] so an MMA B fragment is one 32-bit load.  Each warp owns 16 rows of a tile.
-constexpr int kXs = kIn + 8;  // padded row lengths (halves)
-constexpr int kHs = kH + 8;
-constexpr size_t kPredictSmem = (size_t)(kH * kXs + kH * kHs + 64 * kXs + 64 * kHs) * sizeof(__half) +
-                                (3 * kH + 4) * sizeof(float);
+// ---- fused inference on the 5th-generation tensor cores (tcgen05) ----------------------
+// One CTA of 4 warps runs 128-row tiles: features -> layer 1 -> GELU -> layer 2 -> GELU ->
+// head.  Both layers are M=128, N=128, K=128 products (the 112 inputs zero-padded) issued as
+// eight K=16 tcgen05.mma by one thread, with FP16 operands in shared memory and the FP32
+// accumulator in tensor memory (128 lanes x 128 columns).  Thread t owns tile row t: it
+// builds that row's features, and after each layer reads the row's 128 accumulators with
+// tcgen05.ld (warp w may read lanes 32w..32w+31), so GELU and the head's dot product need
+// no shuffles.  Operand tiles use the 128-byte-swizzled K-major layout: 16-byte chunk j of
+// row r of a 128-row tile sits at (j / 8) x 16 KB + r x 128 + ((j % 8) ^ (r % 8)) x 16.
+// Every wait on the MMA completion barrier is bounded; on a timeout the block sets the
+// error word and leaves, freeing its tensor memory on the way out.
+constexpr int kTileRows = 128;
+constexpr uint32_t kOpBytes = kTileRows * 128 * 2;  // one 128 x 128 fp16 operand tile: 32 KB
+constexpr uint32_t kAtomBytes = kTileRows * 128;    // 64 K-elements (128 B) of all 128 rows: 16 KB
+constexpr uint32_t kTmemCols = 128;
+constexpr uint32_t kSpinLimit = 1u << 22;
+// instruction descriptor, kind::f16: D fp32 (bits 4-5 = 1), A and B fp16 and K-major,
+// N >> 3 at bits 17-22, M >> 4 at bits 24-28
+constexpr uint32_t kIdesc = (1u << 4) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr size_t kPredictSmem = 1024 /* alignment slack */ + 3 * kOpBytes + (3 * kH + 4) * sizeof(float) + 16;
+
+__device__ __forceinline__ uint32_t sw128_chunk(uint32_t r, uint32_t j) {
+    return (j >> 3) * kAtomBytes + r * 128u + (((j & 7u) ^ (r & 7u)) << 4);
+}
+
+// Shared-memory matrix descriptor of a 128-byte-swizzled K-major tile starting at `addr`
+// (1024-byte aligned atom, or an offset of 32 bytes times the K step inside it).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu)  // start address, 16-byte units
+           | ((uint64_t)1u << 16)             // leading byte offset (not used with swizzling)
+           | ((uint64_t)(1024u >> 4) << 32)   // stride byte offset: 8 rows x 128 B
+           | ((uint64_t)1u << 46)             // descriptor version of sm_100
+           | ((uint64_t)2u << 61);            // 128-byte swizzle
+}
+
+// Byte offset of K step k (16 elements) inside an operand tile.
+__device__ __forceinline__ uint32_t kstep_offset(int k) { return (uint32_t)(k >> 2) * kAtomBytes + (uint32_t)(k & 3) * 32u; }
+
+__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %3, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %4, {%5, %5, %5, %5}, p;\n\t}"
+        ::"r"(tmem_d), "l"(a), "l"(b), "r"(accumulate), "r"(kIdesc), "r"(0u));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (uint32_t i = 0; i < kSpinLimit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
+        "[%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ uint32_t pack_half2(float a, float b) {
+    const __half2 h = __floats2half2_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+// Writes W (math layout [in][out], fp16, `in_rows` real inputs) as the B operand: tile row n
+// = output n, K = input, zero beyond in_rows.  Thread t writes row t.
+__device__ __forceinline__ void stage_weights(uint32_t tile, const __half* __restrict__ w, int in_rows, uint32_t t) {
+    for (uint32_t j = 0; j < 16; ++j) {
+        uint32_t q[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int k0 = (int)j * 8 + 2 * e;
+            const float a = k0 < in_rows ? __half2float(w[(size_t)k0 * kH + t]) : 0.0f;
+            const float b = k0 + 1 < in_rows ? __half2float(w[(size_t)(k0 + 1) * kH + t]) : 0.0f;
+            q[e] = pack_half2(a, b);
+        }
+        asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(tile + sw128_chunk(t, j)), "r"(q[0]), "r"(q[1]),
+                     "r"(q[2]), "r"(q[3])
+                     : "memory");
+    }
+}
 
 __global__ void __launch_bounds__(128) predict_kernel(const uint4* __restrict__ st, uint32_t count,
                                                       const __half* __restrict__ w1h, const __half* __restrict__ w2h,
-                                                      const float* __restrict__ params, float* __restrict__ out) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    __half* W1s = reinterpret_cast<__half*>(smem);
-    __half* W2s = W1s + kH * kXs;
-    __half* Xs = W2s + kH * kHs;
-    __half* Hs = Xs + 64 * kXs;
-    float* vec = reinterpret_cast<float*>(Hs + 64 * kHs);  // b1 | b2 | w3 | b3
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
-    for (int e = tid; e < kIn * kH; e += 128) W1s[(e % kH) * kXs + e / kH] = w1h[e];
-    for (int e = tid; e < kH * kH; e += 128) W2s[(e % kH) * kHs + e / kH] = w2h[e];
-    for (int e = tid; e < kH; e += 128) {
+                                                      const float* __restrict__ params, float* __restrict__ out,
+                                                      unsigned* __restrict__ err) {
+    extern __shared__ unsigned char smem_raw[];
+    const uint32_t raw = (uint32_t)__cvta_generic_to_shared(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;  // swizzle atoms need 1024-byte alignment
+    const uint32_t w1s = base, w2s = base + kOpBytes, xs = base + 2 * kOpBytes;
+    float* vec = reinterpret_cast<float*>(smem_raw + (base - raw) + 3 * kOpBytes);  // b1 | b2 | w3 | b3
+    const uint32_t bar = base + 3 * kOpBytes + (3 * kH + 4) * sizeof(float);
+    const uint32_t tmem_slot = bar + 8;
+    const uint32_t t = threadIdx.x, warp = t >> 5;
+
+    stage_weights(w1s, w1h, kIn, t);
+    stage_weights(w2s, w2h, kH, t);
+    for (uint32_t e = t; e < (uint32_t)kH; e += blockDim.x) {
         vec[e] = params[kB1 + e];
         vec[kH + e] = params[kB2 + e];
         vec[2 * kH + e] = params[kW3 + e];
     }
-    if (tid == 0) vec[3 * kH] = params[kB3];
+    if (t == 0) {
+        vec[3 * kH] = params[kB3];
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tmem_slot),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    proxy_fence();
+    tc_fence_before();
     __syncthreads();
-    const int r0 = warp * 16 + g;
-    for (uint32_t tile = blockIdx.x; (uint64_t)tile * 64 < count; tile += gridDim.x) {
-        for (int e = tid; e < 64 * kIn; e += 128) {
-            const int r = e / kIn, j = e % kIn;
-            const uint64_t i = (uint64_t)tile * 64 + r;
-            Xs[r * kXs + j] = __float2half(i < count ? feature(st[i], j) : 0.0f);
-        }
-        __syncthreads();
-        float acc[16][4];
+    tc_fence_after();
+    uint32_t tmem = 0;
+    asm volatile("ld.shared.u32 %0, [%1];" : "=r"(tmem) : "r"(tmem_slot) : "memory");
+    const uint32_t my_lanes = tmem + ((warp * 32u) << 16);
+    uint32_t phase = 0;
+    bool failed = false;
+
+    for (uint32_t tile = blockIdx.x; (uint64_t)tile * kTileRows < count && !failed; tile += gridDim.x) {
+        const uint64_t i = (uint64_t)tile * kTileRows + t;
+        const uint4 s = i < count ? st[i] : make_uint4(0, 0, 0, 0);
+        for (uint32_t j = 0; j < 16; ++j) {  // the row's 128 features (zero for rows past the end)
+            uint32_t q[4];
 #pragma unroll
-        for (int nt = 0; nt < 16; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.0f;
-#pragma unroll
-        for (int ks = 0; ks < kIn; ks += 16) {
-            const uint32_t a0 = *reinterpret_cast<const uint32_t*>(&Xs[r0 * kXs + ks + 2 * t]);
-            const uint32_t a1 = *reinterpret_cast<const uint32_t*>(&Xs[(r0 + 8) * kXs + ks + 2 * t]);
-            const uint32_t a2 = *reinterpret_cast<const uint32_t*>(&Xs[r0 * kXs + ks + 2 * t + 8]);
-            const uint32_t a3 = *reinterpret_cast<const uint32_t*>(&Xs[(r0 + 8) * kXs + ks + 2 * t + 8]);
-#pragma unroll
-            for (int nt = 0; nt < 16; ++nt) {
-                const __half* bp = &W1s[(nt * 8 + g) * kXs + ks + 2 * t];
-                mma16816(acc[nt], a0, a1, a2, a3, *reinterpret_cast<const uint32_t*>(bp),
-                         *reinterpret_cast<const uint32_t*>(bp + 8));
+            for (int e = 0; e < 4; ++e) {
+                const int k0 = (int)j * 8 + 2 * e;
+                q[e] = i < count ? pack_half2(feature(s, k0), feature(s, k0 + 1)) : 0u;
             }
+            asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(xs + sw128_chunk(t, j)), "r"(q[0]),
+                         "r"(q[1]), "r"(q[2]), "r"(q[3])
+                         : "memory");
         }
+        float sum = 0.0f;
+        for (int layer = 0; layer < 2 && !failed; ++layer) {
+            proxy_fence();  // make the operand tile visible to the tensor cores
+            tc_fence_before();
+            __syncthreads();
+            if (t == 0) {
+                tc_fence_after();
+                const uint32_t wt = layer == 0 ? w1s : w2s;
 #pragma unroll
-        for (int nt = 0; nt < 16; ++nt)
+                for (int k = 0; k < 8; ++k)
+                    umma_f16(tmem, sw128_desc(xs + kstep_offset(k)), sw128_desc(wt + kstep_offset(k)), k > 0 ? 1u : 0u);
+                umma_commit(bar);
+            }
+            const bool ok = mbar_wait(bar, phase);
+            phase ^= 1u;
+            failed = __syncthreads_or(!ok) != 0;
+            if (failed) break;
+            tc_fence_after();
+            const float* bias = vec + layer * kH;
+            for (uint32_t c = 0; c < (uint32_t)kH; c += 16) {
+                float v[16];
+                tmem_ld16(my_lanes + c, v);
+                if (layer == 0) {  // H1 = gelu(Z1 + b1), fp16, becomes the A operand of layer 2
+                    uint32_t q[8];
 #pragma unroll
-            for (int h = 0; h < 2; ++h)
+                    for (int e = 0; e < 8; ++e)
+                        q[e] = pack_half2(gelu(v[2 * e] + bias[c + 2 * e]), gelu(v[2 * e + 1] + bias[c + 2 * e + 1]));
+                    asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(xs + sw128_chunk(t, c / 8)),
+                                 "r"(q[0]), "r"(q[1]), "r"(q[2]), "r"(q[3])
+                                 : "memory");
+                    asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(xs + sw128_chunk(t, c / 8 + 1)),
+                                 "r"(q[4]), "r"(q[5]), "r"(q[6]), "r"(q[7])
+                                 : "memory");
+                } else {  // head: H2 rounded to fp16 as in the training forward pass
 #pragma unroll
-                for (int c = 0; c < 2; ++c) {
-                    const int j = nt * 8 + 2 * t + c;
-                    Hs[(r0 + 8 * h) * kHs + j] = __float2half(gelu(acc[nt][2 * h + c] + vec[j]));
+                    for (int e = 0; e < 16; ++e)
+                        sum += __half2float(__float2half(gelu(v[e] + bias[c + e]))) * vec[2 * kH + c + e];
                 }
-        __syncwarp();
-#pragma unroll
-        for (int nt = 0; nt < 16; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.0f;
-#pragma unroll
-        for (int ks = 0; ks < kH; ks += 16) {
-            const uint32_t a0 = *reinterpret_cast<const uint32_t*>(&Hs[r0 * kHs + ks + 2 * t]);
-            const uint32_t a1 = *reinterpret_cast<const uint32_t*>(&Hs[(r0 + 8) * kHs + ks + 2 * t]);
-            const uint32_t a2 = *reinterpret_cast<const uint32_t*>(&Hs[r0 * kHs + ks + 2 * t + 8]);
-            const uint32_t a3 = *reinterpret_cast<const uint32_t*>(&Hs[(r0 + 8) * kHs + ks + 2 * t + 8]);
-#pragma unroll
-            for (int nt = 0; nt < 16; ++nt) {
-                const __half* bp = &W2s[(nt * 8 + g) * kHs + ks + 2 * t];
-                mma16816(acc[nt], a0, a1, a2, a3, *reinterpret_cast<const uint32_t*>(bp),
-                         *reinterpret_cast<const uint32_t*>(bp + 8));
             }
+            tc_fence_before();
         }
-        float s0 = 0.0f, s1 = 0.0f;
-#pragma unroll
-        for (int nt = 0; nt < 16; ++nt)
-#pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                const int j = nt * 8 + 2 * t + c;
-                // H2 rounded to fp16 as in the training forward pass (head_kernel reads fp16 H2)
-                s0 += __half2float(__float2half(gelu(acc[nt][c] + vec[kH + j]))) * vec[2 * kH + j];
-                s1 += __half2float(__float2half(gelu(acc[nt][2 + c] + vec[kH + j]))) * vec[2 * kH + j];
-            }
-        s0 += __shfl_xor_sync(0xFFFFFFFFu, s0, 1);
-        s0 += __shfl_xor_sync(0xFFFFFFFFu, s0, 2);
-        s1 += __shfl_xor_sync(0xFFFFFFFFu, s1, 1);
-        s1 += __shfl_xor_sync(0xFFFFFFFFu, s1, 2);
-        if (t == 0) {
-            const uint64_t i = (uint64_t)tile * 64 + r0;
-            if (i < count) out[i] = s0 + vec[3 * kH];
-            if (i + 8 < count) out[i + 8] = s1 + vec[3 * kH];
-        }
-        __syncthreads();
+        if (!failed && i < count) out[i] = sum + vec[3 * kH];
+        __syncthreads();  // the operand tile and the accumulator are free for the next tile
+    }
+    if (failed && t == 0) atomicOr(err, 1u);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
     }
 }
 
@@ -662,11 +774,23 @@ int model_predict_device(const nqb_model* m, const nqb_state* d_states, uint32_t
     if (e != cudaSuccess) return cuda_status(e);
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device);
-    const uint64_t tiles = (count + 63) / 64;
+    const uint64_t tiles = (count + kTileRows - 1) / kTileRows;
+    // at most 2 blocks per SM (shared memory), so their tensor memory (2 x 128 columns) fits
     const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(tiles, (uint64_t)sms * 2));
-    predict_kernel<<<grid, 128, kPredictSmem, s>>>(reinterpret_cast<const uint4*>(d_states), count, m->w1h, m->w2h,
-                                                   m->params, d_out);
-    return cuda_status(cudaGetLastError());
+    unsigned* d_err = nullptr;
+    NQB_TRY(dev_alloc(&d_err, sizeof(unsigned), s));
+    unsigned h_err = 0;
+    int st = cuda_status(cudaMemsetAsync(d_err, 0, sizeof(unsigned), s));
+    if (!st) {
+        predict_kernel<<<grid, kTileRows, kPredictSmem, s>>>(reinterpret_cast<const uint4*>(d_states), count, m->w1h,
+                                                             m->w2h, m->params, d_out, d_err);
+        st = cuda_status(cudaGetLastError());
+    }
+    if (!st) st = cuda_status(cudaMemcpyAsync(&h_err, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    if (!st) st = cuda_status(cudaStreamSynchronize(s));
+    dev_free(d_err, s);
+    if (!st && h_err) st = NQB_E_STALL;
+    return st;
 }
 
 int model_device(const nqb_model* m) { return m->device; }

@@ -141,3 +141,14 @@ def test_learned_schedule_beats_fifo_on_coarse_pool(nqb, trained):
 def test_no_split_rounds_still_exact(nqb, trained):
     c, st = nqb.count_ex(15, 2, form=1, model=trained, max_split_rounds=0)
     assert c == KAT[15]
+
+
+@pytest.mark.gpu
+def test_predict_many_tiles(nqb, model):
+    """Enough boards for several 128-row tiles per persistent block (the completion barrier
+    changes phase twice per tile), checked row by row against the CPU forward pass."""
+    boards = nqb.sample_boards(77, 200_000, 8, 22, 1, 7)
+    y = model.predict(boards)
+    want, _ = mlp_ref.forward(model.get_params().astype(np.float64), mlp_ref.features(boards))
+    assert np.max(np.abs(y - want)) < 2e-3 * max(1.0, np.max(np.abs(want)))
+    assert np.array_equal(model.predict(boards[:1]), y[:1])  # a single, partial tile
