@@ -26,69 +26,222 @@ namespace nqb {
 namespace mlp {
 namespace {
 
-// ---- generic GEMM: C (M x N, fp32, row-major ldc) = alpha * A x B + beta * C -----------
-// A(i, k) = A[i * sai + k * sak], B(k, j) = B[k * sbk + j * sbj], fp16.  Block tile 64 x 64,
-// 4 warps, each 16 rows x 64 columns (8 MMA n-tiles); K in steps of 16.
-constexpr int kTile = 64;
-constexpr int kKs = 16;
-constexpr int kPad = 8;  // row padding (halves) that keeps fragment loads conflict-free
+// ---- tcgen05 building blocks -----------------------------------------------------------
+// Operand tiles are 128 rows x K fp16 in the 128-byte-swizzled K-major layout: 16-byte
+// chunk j (8 K-elements) of row r sits at (j / 8) x 16 KB + r x 128 + ((j % 8) ^ (r % 8)) x 16
+// from a 1024-byte-aligned base.  One thread issues the MMAs; the accumulator lives in
+// tensor memory and each warp reads its 32 lanes back with tcgen05.ld.
+constexpr int kTileRows = 128;
+constexpr uint32_t kOpBytes = kTileRows * 128 * 2;  // one 128 x 128 fp16 operand tile: 32 KB
+constexpr uint32_t kAtomBytes = kTileRows * 128;    // 64 K-elements (128 B) of all 128 rows: 16 KB
+constexpr uint32_t kTmemCols = 128;
+constexpr uint32_t kSpinLimit = 1u << 22;
+// instruction descriptor, kind::f16: D fp32 (bits 4-5 = 1), A and B fp16 and K-major,
+// N >> 3 at bits 17-22, M >> 4 at bits 24-28
+constexpr uint32_t kIdesc = (1u << 4) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr size_t kPredictSmem = 1024 /* alignment slack */ + 3 * kOpBytes + (3 * kH + 4) * sizeof(float) + 16;
 
-__global__ void __launch_bounds__(128) gemm_f16(const __half* __restrict__ A, long sai, long sak,
-                                                const __half* __restrict__ B, long sbk, long sbj,
-                                                float* __restrict__ C, long ldc, int M, int N, int K, float alpha,
-                                                float beta) {
-    __shared__ __align__(16) __half As[kTile][kKs + kPad];
-    __shared__ __align__(16) __half Bs[kTile][kKs + kPad];  // [n][k]
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int g = lane >> 2, t = lane & 3;
-    const int bm = blockIdx.y * kTile, bn = blockIdx.x * kTile;
-    float acc[8][4];
+__device__ __forceinline__ uint32_t sw128_chunk(uint32_t r, uint32_t j) {
+    return (j >> 3) * kAtomBytes + r * 128u + (((j & 7u) ^ (r & 7u)) << 4);
+}
+
+// Shared-memory matrix descriptor of a 128-byte-swizzled K-major tile starting at `addr`
+// (1024-byte aligned atom, or an offset of 32 bytes times the K step inside it).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu)  // start address, 16-byte units
+           | ((uint64_t)1u << 16)             // leading byte offset (not used with swizzling)
+           | ((uint64_t)(1024u >> 4) << 32)   // stride byte offset: 8 rows x 128 B
+           | ((uint64_t)1u << 46)             // descriptor version of sm_100
+           | ((uint64_t)2u << 61);            // 128-byte swizzle
+}
+
+// Byte offset of K step k (16 elements) inside an operand tile.
+__device__ __forceinline__ uint32_t kstep_offset(int k) { return (uint32_t)(k >> 2) * kAtomBytes + (uint32_t)(k & 3) * 32u; }
+
+__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %3, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %4, {%5, %5, %5, %5}, p;\n\t}"
+        ::"r"(tmem_d), "l"(a), "l"(b), "r"(accumulate), "r"(kIdesc), "r"(0u));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (uint32_t i = 0; i < kSpinLimit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
+        "[%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-    for (int i = 0; i < 8; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.0f;
-    for (int k0 = 0; k0 < K; k0 += kKs) {
-        for (int e = tid; e < kTile * kKs; e += 128) {
-            const int r = e / kKs, kk = e % kKs;
-            const int gi = bm + r, gj = bn + r, gk = k0 + kk;
-            As[r][kk] = (gi < M && gk < K) ? A[gi * sai + gk * sak] : __float2half(0.0f);
-            Bs[r][kk] = (gj < N && gk < K) ? B[gk * sbk + gj * sbj] : __float2half(0.0f);
-        }
-        __syncthreads();
-        const int r0 = warp * 16 + g;
-        const uint32_t a0 = *reinterpret_cast<const uint32_t*>(&As[r0][2 * t]);
-        const uint32_t a1 = *reinterpret_cast<const uint32_t*>(&As[r0 + 8][2 * t]);
-        const uint32_t a2 = *reinterpret_cast<const uint32_t*>(&As[r0][2 * t + 8]);
-        const uint32_t a3 = *reinterpret_cast<const uint32_t*>(&As[r0 + 8][2 * t + 8]);
-#pragma unroll
-        for (int nt = 0; nt < 8; ++nt) {
-            const uint32_t b0 = *reinterpret_cast<const uint32_t*>(&Bs[nt * 8 + g][2 * t]);
-            const uint32_t b1 = *reinterpret_cast<const uint32_t*>(&Bs[nt * 8 + g][2 * t + 8]);
-            mma16816(acc[nt], a0, a1, a2, a3, b0, b1);
-        }
-        __syncthreads();
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ uint32_t pack_half2(float a, float b) {
+    const __half2 h = __floats2half2_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+// ---- GEMM: C (M x N, fp32, row-major ldc) = alpha * A x B, on tcgen05 ----------------------
+// A(i, k) = A[i * sai + k * sak], B(k, j) = B[k * sbk + j * sbj], fp16; N <= 128.  A block
+// owns 128 rows of C and a range of K; every 64-element K step is loaded into swizzled
+// shared memory (a 16-byte vector per chunk when K is contiguous and aligned, else 8
+// element loads that are coalesced across the block's rows) and multiplied as four K=16
+// MMAs into a 128 x 128 fp32 tensor-memory accumulator.  With several K ranges (the weight
+// gradients, K = batch rows) each block adds its partial product with fp32 atomics into a
+// zeroed C.  The shared-memory request caps residency at 3 blocks (384 tensor-memory
+// columns) per SM.
+constexpr uint32_t kGemmSmem = 72 * 1024;
+constexpr int kGemmK = 64;
+
+__device__ __forceinline__ void load_chunk(const __half* __restrict__ p, long stride_k, int valid, bool vec,
+                                           uint32_t q[4]) {
+    if (vec && valid == 8) {
+        const uint4 v = *reinterpret_cast<const uint4*>(p);
+        q[0] = v.x, q[1] = v.y, q[2] = v.z, q[3] = v.w;
+        return;
     }
 #pragma unroll
-    for (int nt = 0; nt < 8; ++nt) {
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int i = bm + warp * 16 + g + 8 * h;
-            if (i >= M) continue;
-#pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                const int j = bn + nt * 8 + 2 * t + c;
-                if (j >= N) continue;
-                float* p = C + (long)i * ldc + j;
-                const float v = alpha * acc[nt][2 * h + c];
-                *p = beta == 0.0f ? v : v + beta * *p;
-            }
-        }
+    for (int e = 0; e < 4; ++e) {
+        const __half a = 2 * e < valid ? p[(long)(2 * e) * stride_k] : __float2half(0.0f);
+        const __half b = 2 * e + 1 < valid ? p[(long)(2 * e + 1) * stride_k] : __float2half(0.0f);
+        __half2 h = __halves2half2(a, b);
+        q[e] = *reinterpret_cast<const uint32_t*>(&h);
     }
 }
 
+__global__ void __launch_bounds__(128) gemm_tc(const __half* __restrict__ A, long sai, long sak, bool a_vec,
+                                               const __half* __restrict__ B, long sbk, long sbj, bool b_vec,
+                                               float* __restrict__ C, long ldc, int M, int N, int K, int k_per_block,
+                                               float alpha, bool atomic, unsigned* __restrict__ err) {
+    extern __shared__ unsigned char smem_raw[];
+    const uint32_t raw = (uint32_t)__cvta_generic_to_shared(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    const uint32_t as = base, bs = base + kAtomBytes, bar = base + 2 * kAtomBytes, tmem_slot = bar + 8;
+    const uint32_t t = threadIdx.x, warp = t >> 5;
+    const int m0 = blockIdx.x * kTileRows;
+    const int kb = blockIdx.y * k_per_block, ke = min(K, kb + k_per_block);
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tmem_slot),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    uint32_t tmem = 0;
+    asm volatile("ld.shared.u32 %0, [%1];" : "=r"(tmem) : "r"(tmem_slot) : "memory");
+    uint32_t phase = 0;
+    bool failed = false;
+    const int i = m0 + (int)t;  // this thread's row of A and of C
+    const int j = (int)t;       // this thread's row of B (column of C)
+    for (int k0 = kb; k0 < ke && !failed; k0 += kGemmK) {
+#pragma unroll
+        for (uint32_t c = 0; c < kGemmK / 8; ++c) {
+            const int k = k0 + (int)c * 8;
+            const int valid = max(0, min(8, ke - k));
+            uint32_t q[4] = {0u, 0u, 0u, 0u};
+            if (i < M) load_chunk(A + (long)i * sai + (long)k * sak, sak, valid, a_vec, q);
+            asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(as + sw128_chunk(t, c)), "r"(q[0]),
+                         "r"(q[1]), "r"(q[2]), "r"(q[3])
+                         : "memory");
+            q[0] = q[1] = q[2] = q[3] = 0u;
+            if (j < N) load_chunk(B + (long)k * sbk + (long)j * sbj, sbk, valid, b_vec, q);
+            asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(bs + sw128_chunk(t, c)), "r"(q[0]),
+                         "r"(q[1]), "r"(q[2]), "r"(q[3])
+                         : "memory");
+        }
+        proxy_fence();
+        tc_fence_before();
+        __syncthreads();
+        if (t == 0) {
+            tc_fence_after();
+#pragma unroll
+            for (int ks = 0; ks < 4; ++ks)
+                umma_f16(tmem, sw128_desc(as + ks * 32u), sw128_desc(bs + ks * 32u), (k0 > kb || ks > 0) ? 1u : 0u);
+            umma_commit(bar);
+        }
+        const bool ok = mbar_wait(bar, phase);
+        phase ^= 1u;
+        failed = __syncthreads_or(!ok) != 0;  // the shared tiles are free again once the MMAs are done
+    }
+    if (!failed && kb < ke) {
+        tc_fence_after();
+        const uint32_t my_lanes = tmem + ((warp * 32u) << 16);
+        for (int c = 0; c < 128; c += 16) {
+            float v[16];
+            tmem_ld16(my_lanes + (uint32_t)c, v);
+            if (i < M) {
+#pragma unroll
+                for (int e = 0; e < 16; ++e) {
+                    const int col = c + e;
+                    if (col >= N) continue;
+                    float* p = C + (long)i * ldc + col;
+                    if (atomic) atomicAdd(p, alpha * v[e]);
+                    else *p = alpha * v[e];
+                }
+            }
+        }
+    }
+    if (failed && t == 0) atomicOr(err, 1u);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+    }
+}
+
+// C = alpha * A x B (the only form training uses; beta must be 0).  `err`: device word the
+// kernel sets when an MMA completion wait times out.
 int gemm(const __half* A, long sai, long sak, const __half* B, long sbk, long sbj, float* C, long ldc, int M, int N,
-         int K, float alpha, float beta, cudaStream_t s) {
+         int K, float alpha, float beta, unsigned* err, cudaStream_t s) {
     if (M <= 0 || N <= 0 || K <= 0) return NQB_OK;
-    const dim3 grid((N + kTile - 1) / kTile, (M + kTile - 1) / kTile);
-    gemm_f16<<<grid, 128, 0, s>>>(A, sai, sak, B, sbk, sbj, C, ldc, M, N, K, alpha, beta);
+    if (beta != 0.0f || N > 128) return NQB_E_INVALID;
+    NQB_TRY(cuda_status(cudaFuncSetAttribute(gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem)));
+    auto vec_ok = [](const __half* p, long s_row, long s_k) {
+        return s_k == 1 && ((uintptr_t)p & 15u) == 0 && (s_row * (long)sizeof(__half)) % 16 == 0;
+    };
+    const bool a_vec = vec_ok(A, sai, sak), b_vec = vec_ok(B, sbj, sbk);
+    const int m_tiles = (M + kTileRows - 1) / kTileRows;
+    // split K when it is long (the weight gradients): at least 256 K per block
+    int splits = 1;
+    if (K > 256) splits = std::min((K + 255) / 256, std::max(1, 148 * 3 / m_tiles));
+    const int per = ((K + splits - 1) / splits + kGemmK - 1) / kGemmK * kGemmK;
+    splits = (K + per - 1) / per;
+    if (splits > 1)  // partial products are added into a zeroed C
+        NQB_TRY(cuda_status(
+            cudaMemset2DAsync(C, (size_t)ldc * sizeof(float), 0, (size_t)N * sizeof(float), (size_t)M, s)));
+    const dim3 grid(m_tiles, splits);
+    gemm_tc<<<grid, kTileRows, kGemmSmem, s>>>(A, sai, sak, a_vec, B, sbk, sbj, b_vec, C, ldc, M, N, K, per, alpha,
+                                              splits > 1, err);
     return cuda_status(cudaGetLastError());
 }
 
@@ -222,79 +375,6 @@ __global__ void to_half_kernel(const float* __restrict__ p, __half* __restrict__
 // row r of a 128-row tile sits at (j / 8) x 16 KB + r x 128 + ((j % 8) ^ (r % 8)) x 16.
 // Every wait on the MMA completion barrier is bounded; on a timeout the block sets the
 // error word and leaves, freeing its tensor memory on the way out.
-constexpr int kTileRows = 128;
-constexpr uint32_t kOpBytes = kTileRows * 128 * 2;  // one 128 x 128 fp16 operand tile: 32 KB
-constexpr uint32_t kAtomBytes = kTileRows * 128;    // 64 K-elements (128 B) of all 128 rows: 16 KB
-constexpr uint32_t kTmemCols = 128;
-constexpr uint32_t kSpinLimit = 1u << 22;
-// instruction descriptor, kind::f16: D fp32 (bits 4-5 = 1), A and B fp16 and K-major,
-// N >> 3 at bits 17-22, M >> 4 at bits 24-28
-constexpr uint32_t kIdesc = (1u << 4) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
-constexpr size_t kPredictSmem = 1024 /* alignment slack */ + 3 * kOpBytes + (3 * kH + 4) * sizeof(float) + 16;
-
-__device__ __forceinline__ uint32_t sw128_chunk(uint32_t r, uint32_t j) {
-    return (j >> 3) * kAtomBytes + r * 128u + (((j & 7u) ^ (r & 7u)) << 4);
-}
-
-// Shared-memory matrix descriptor of a 128-byte-swizzled K-major tile starting at `addr`
-// (1024-byte aligned atom, or an offset of 32 bytes times the K step inside it).
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
-    return (uint64_t)((addr >> 4) & 0x3FFFu)  // start address, 16-byte units
-           | ((uint64_t)1u << 16)             // leading byte offset (not used with swizzling)
-           | ((uint64_t)(1024u >> 4) << 32)   // stride byte offset: 8 rows x 128 B
-           | ((uint64_t)1u << 46)             // descriptor version of sm_100
-           | ((uint64_t)2u << 61);            // 128-byte swizzle
-}
-
-// Byte offset of K step k (16 elements) inside an operand tile.
-__device__ __forceinline__ uint32_t kstep_offset(int k) { return (uint32_t)(k >> 2) * kAtomBytes + (uint32_t)(k & 3) * 32u; }
-
-__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %3, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %4, {%5, %5, %5, %5}, p;\n\t}"
-        ::"r"(tmem_d), "l"(a), "l"(b), "r"(accumulate), "r"(kIdesc), "r"(0u));
-}
-
-__device__ __forceinline__ void umma_commit(uint32_t bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-    for (uint32_t i = 0; i < kSpinLimit; ++i) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(bar), "r"(parity)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
-
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
-        "[%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-__device__ __forceinline__ uint32_t pack_half2(float a, float b) {
-    const __half2 h = __floats2half2_rn(a, b);
-    return *reinterpret_cast<const uint32_t*>(&h);
-}
-
 // Writes W (math layout [in][out], fp16, `in_rows` real inputs) as the B operand: tile row n
 // = output n, K = input, zero beyond in_rows.  Thread t writes row t.
 __device__ __forceinline__ void stage_weights(uint32_t tile, const __half* __restrict__ w, int in_rows, uint32_t t) {
@@ -426,6 +506,7 @@ struct Work {
     __half *X = nullptr, *H1 = nullptr, *H2 = nullptr, *dZ2 = nullptr, *dZ1 = nullptr;
     float *t = nullptr, *Z = nullptr, *Zb1 = nullptr, *Zb2 = nullptr, *y = nullptr, *dy = nullptr, *dH1 = nullptr,
           *loss = nullptr;
+    unsigned* err = nullptr;  // set by a GEMM whose tensor-core completion wait timed out
     uint32_t cap = 0;
     std::vector<void*> owned;
 
@@ -455,7 +536,16 @@ struct Work {
         if (!s) s = get(&dy, r * sizeof(float));
         if (!s) s = get(&dH1, r * kH * sizeof(float));
         if (!s) s = get(&loss, sizeof(float));
+        if (!s) s = get(&err, sizeof(unsigned));
+        if (!s) s = cuda_status(cudaMemset(err, 0, sizeof(unsigned)));
         return s;
+    }
+    // NQB_E_STALL if a GEMM of the passes so far timed out (synchronises the stream).
+    int check(cudaStream_t s) const {
+        unsigned h = 0;
+        int st = cuda_status(cudaMemcpyAsync(&h, err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+        if (!st) st = cuda_status(cudaStreamSynchronize(s));
+        return st ? st : (h ? NQB_E_STALL : NQB_OK);
     }
     ~Work() {
         for (void* p : owned) cudaFree(p);
@@ -492,9 +582,9 @@ int pass(nqb_model* m, Work& w, uint32_t rows, cudaStream_t s) {
     int st;
     cudaMemsetAsync(G, 0, kParams * sizeof(float), s);
     // forward
-    if ((st = gemm(w.X, kIn, 1, m->w1h, kH, 1, w.Z, kH, rows, kH, kIn, 1.0f, 0.0f, s))) return st;
+    if ((st = gemm(w.X, kIn, 1, m->w1h, kH, 1, w.Z, kH, rows, kH, kIn, 1.0f, 0.0f, w.err, s))) return st;
     bias_gelu_kernel<<<blocks_for((uint64_t)rows * kH), 256, 0, s>>>(w.Z, P + kB1, rows, w.Zb1, w.H1);
-    if ((st = gemm(w.H1, kH, 1, m->w2h, kH, 1, w.Z, kH, rows, kH, kH, 1.0f, 0.0f, s))) return st;
+    if ((st = gemm(w.H1, kH, 1, m->w2h, kH, 1, w.Z, kH, rows, kH, kH, 1.0f, 0.0f, w.err, s))) return st;
     bias_gelu_kernel<<<blocks_for((uint64_t)rows * kH), 256, 0, s>>>(w.Z, P + kB2, rows, w.Zb2, w.H2);
     head_kernel<<<blocks_for((uint64_t)rows * 32), 256, 0, s>>>(w.H2, P + kW3, P + kB3, rows, w.y);
     loss_kernel<<<blocks_for(rows), 256, 0, s>>>(w.y, w.t, rows, w.dy, w.loss);
@@ -505,13 +595,13 @@ int pass(nqb_model* m, Work& w, uint32_t rows, cudaStream_t s) {
     dz2_kernel<<<blocks_for((uint64_t)rows * kH), 256, 0, s>>>(w.dy, P + kW3, w.Zb2, rows, w.dZ2);
     colsum_kernel<<<std::min<unsigned>(rows, 512), kH, 0, s>>>(w.dZ2, nullptr, rows, inv, G + kB2);
     // dW2 = H1^T dZ2: A(i, k) = H1[k][i], B(k, j) = dZ2[k][j]
-    if ((st = gemm(w.H1, 1, kH, w.dZ2, kH, 1, G + kW2, kH, kH, kH, rows, inv, 0.0f, s))) return st;
+    if ((st = gemm(w.H1, 1, kH, w.dZ2, kH, 1, G + kW2, kH, kH, kH, rows, inv, 0.0f, w.err, s))) return st;
     // dH1 = dZ2 W2^T: B(k, j) = W2[j][k]
-    if ((st = gemm(w.dZ2, kH, 1, m->w2h, 1, kH, w.dH1, kH, rows, kH, kH, 1.0f, 0.0f, s))) return st;
+    if ((st = gemm(w.dZ2, kH, 1, m->w2h, 1, kH, w.dH1, kH, rows, kH, kH, 1.0f, 0.0f, w.err, s))) return st;
     dz1_kernel<<<blocks_for((uint64_t)rows * kH), 256, 0, s>>>(w.dH1, w.Zb1, rows, w.dZ1);
     colsum_kernel<<<std::min<unsigned>(rows, 512), kH, 0, s>>>(w.dZ1, nullptr, rows, inv, G + kB1);
     // dW1 = X^T dZ1
-    if ((st = gemm(w.X, 1, kIn, w.dZ1, kH, 1, G + kW1, kH, kIn, kH, rows, inv, 0.0f, s))) return st;
+    if ((st = gemm(w.X, 1, kIn, w.dZ1, kH, 1, G + kW1, kH, kIn, kH, rows, inv, 0.0f, w.err, s))) return st;
     return cuda_status(cudaGetLastError());
 }
 
@@ -695,7 +785,7 @@ int nqb_model_loss_grad(nqb_model* m, const nqb_state* states, const float* targ
     float l = 0;
     st = cuda_status(cudaMemcpyAsync(&l, w.loss, sizeof(float), cudaMemcpyDeviceToHost, cs.s));
     if (!st) st = cuda_status(cudaMemcpyAsync(grad, m->grad, kParams * sizeof(float), cudaMemcpyDeviceToHost, cs.s));
-    if (!st) st = cuda_status(cudaStreamSynchronize(cs.s));
+    if (!st) st = w.check(cs.s);
     *loss = l / (float)count;
     return st;
 }
@@ -757,7 +847,7 @@ int nqb_model_train(nqb_model* m, const nqb_state* states, const float* targets,
         }
         float l = 0;
         st = cuda_status(cudaMemcpyAsync(&l, w.loss, sizeof(float), cudaMemcpyDeviceToHost, cs.s));
-        if (!st) st = cuda_status(cudaStreamSynchronize(cs.s));
+        if (!st) st = w.check(cs.s);
         if (st) return st;
         if (epoch_loss) epoch_loss[ep] = l / (float)count;
     }

@@ -1,5 +1,5 @@
-// Learned cost model: shapes, feature encoding and the tensor-core fragment helpers shared by
-// the training kernels (mlp.cu) and the fused inference kernel.  Device and host.
+// Learned cost model: shapes, the feature encoding and the activation shared by the training
+// kernels (mlp.cu), the fused inference kernel and the host.  Device and host.
 #pragma once
 
 #include <cstdint>
@@ -57,20 +57,6 @@ __host__ __device__ __forceinline__ float feature(const uint4 st, int j) {
 #endif
         default: return 0.0f;
     }
-}
-
-// One m16n8k16 tensor-core MMA: D(16x8, f32) += A(16x16, f16, row) x B(16x8, f16, col).
-// Fragment ownership (g = lane / 4, t = lane % 4):
-//   a0 = A[g][2t..2t+1]      a1 = A[g+8][2t..2t+1]   a2 = A[g][2t+8..]   a3 = A[g+8][2t+8..]
-//   b0 = B[2t..2t+1][g]      b1 = B[2t+8..2t+9][g]
-//   c0,c1 = D[g][2t..2t+1]   c2,c3 = D[g+8][2t..2t+1]
-__device__ __forceinline__ void mma16816(float c[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
-                                         uint32_t b0, uint32_t b1) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
-        "{%0, %1, %2, %3};"
-        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
 __device__ __forceinline__ uint32_t pack_half2(__half lo, __half hi) {
