@@ -193,21 +193,31 @@ __global__ void __launch_bounds__(128) gemm_tc(const __half* __restrict__ A, lon
         failed = __syncthreads_or(!ok) != 0;  // the shared tiles are free again once the MMAs are done
     }
     if (!failed && kb < ke) {
+        // Epilogue: 32 accumulator columns at a time go through shared memory (the operand
+        // tiles are free now), [128 rows][33 floats], so that a warp then writes 32
+        // consecutive floats of one row of C per store.
         tc_fence_after();
         const uint32_t my_lanes = tmem + ((warp * 32u) << 16);
-        for (int c = 0; c < 128; c += 16) {
-            float v[16];
-            tmem_ld16(my_lanes + (uint32_t)c, v);
-            if (i < M) {
+        float* stage = reinterpret_cast<float*>(smem_raw + (base - raw));
+        constexpr int kLd = 33;  // padded row: column reads of the staging tile avoid bank conflicts
+        for (int c0 = 0; c0 < 128; c0 += 32) {
+            float v[32];
+            tmem_ld16(my_lanes + (uint32_t)c0, v);
+            tmem_ld16(my_lanes + (uint32_t)c0 + 16u, v + 16);
 #pragma unroll
-                for (int e = 0; e < 16; ++e) {
-                    const int col = c + e;
-                    if (col >= N) continue;
-                    float* p = C + (long)i * ldc + col;
-                    if (atomic) atomicAdd(p, alpha * v[e]);
-                    else *p = alpha * v[e];
+            for (int e = 0; e < 32; ++e) stage[t * kLd + e] = v[e];
+            __syncthreads();
+            const int lane = (int)(t & 31u), col = c0 + lane;
+            for (int r = (int)warp; r < kTileRows; r += 4) {
+                const int row = m0 + r;
+                if (row < M && col < N) {
+                    float* p = C + (long)row * ldc + col;
+                    const float x = alpha * stage[r * kLd + lane];
+                    if (atomic) atomicAdd(p, x);
+                    else *p = x;
                 }
             }
+            __syncthreads();
         }
     }
     if (failed && t == 0) atomicOr(err, 1u);
