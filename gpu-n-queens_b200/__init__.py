@@ -426,6 +426,7 @@ def _model_sigs(L):
         "nqb_model_set_params": (ctypes.c_int, [vp, vp]),
         "nqb_model_features": (ctypes.c_int, [vp, ctypes.c_uint64, vp]),
         "nqb_model_predict": (ctypes.c_int, [vp, vp, ctypes.c_uint64, vp]),
+        "nqb_model_predict_ex": (ctypes.c_int, [vp, vp, ctypes.c_uint64, vp, ctypes.c_uint32]),
         "nqb_model_loss_grad": (ctypes.c_int, [vp, vp, vp, ctypes.c_uint64, fp, vp]),
         "nqb_model_train": (ctypes.c_int, [vp, vp, vp, ctypes.c_uint64, ctypes.POINTER(TrainOpts), vp]),
         "nqb_record_nodes": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.POINTER(Opts), vp, vp]),
@@ -466,11 +467,13 @@ class Model:
         assert p.size == MODEL_PARAMS
         _check(lib().nqb_model_set_params(self.handle, p.ctypes.data), "nqb_model_set_params")
 
-    def predict(self, states):
+    def predict(self, states, wait_limit=0):
+        """Predicted log2(1 + nodes) per state.  wait_limit bounds each tensor-core completion
+        wait (0: the library default); a wait that runs out raises NQBError(E_STALL)."""
         states = np.ascontiguousarray(states, dtype=STATE_DTYPE)
         out = np.zeros(max(len(states), 1), dtype=np.float32)
-        _check(lib().nqb_model_predict(self.handle, states.ctypes.data, len(states), out.ctypes.data),
-               "nqb_model_predict")
+        _check(lib().nqb_model_predict_ex(self.handle, states.ctypes.data, len(states), out.ctypes.data, wait_limit),
+               "nqb_model_predict_ex")
         return out[:len(states)]
 
     def loss_grad(self, states, targets):

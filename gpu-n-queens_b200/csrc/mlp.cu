@@ -35,7 +35,7 @@ constexpr int kTileRows = 128;
 constexpr uint32_t kOpBytes = kTileRows * 128 * 2;  // one 128 x 128 fp16 operand tile: 32 KB
 constexpr uint32_t kAtomBytes = kTileRows * 128;    // 64 K-elements (128 B) of all 128 rows: 16 KB
 constexpr uint32_t kTmemCols = 128;
-constexpr uint32_t kSpinLimit = 1u << 22;
+constexpr uint32_t kSpinLimit = 1u << 22;  // waits: far above the ~1 us a product takes
 // instruction descriptor, kind::f16: D fp32 (bits 4-5 = 1), A and B fp16 and K-major,
 // N >> 3 at bits 17-22, M >> 4 at bits 24-28
 constexpr uint32_t kIdesc = (1u << 4) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
@@ -69,14 +69,28 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-    for (uint32_t i = 0; i < kSpinLimit; ++i) {
+// Bounded wait for a phase of the completion barrier.  By default mbarrier.try_wait, which
+// may suspend the thread until the phase completes (no issue slots burnt while the tensor
+// cores work); with probe_only, `limit` non-blocking mbarrier.test_wait probes, an exact
+// count whatever the hardware's suspend time (a caller-chosen bound).
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint32_t limit = kSpinLimit,
+                                          bool probe_only = false) {
+    for (uint32_t i = 0; i < limit; ++i) {
         uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(bar), "r"(parity)
-            : "memory");
+        if (probe_only)
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                "selp.u32 %0, 1, 0, p;\n\t}"
+                : "=r"(done)
+                : "r"(bar), "r"(parity)
+                : "memory");
+        else
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                "selp.u32 %0, 1, 0, p;\n\t}"
+                : "=r"(done)
+                : "r"(bar), "r"(parity)
+                : "memory");
         if (done) return true;
     }
     return false;
@@ -189,8 +203,12 @@ __global__ void __launch_bounds__(128) gemm_tc(const __half* __restrict__ A, lon
             umma_commit(bar);
         }
         const bool ok = mbar_wait(bar, phase);
-        phase ^= 1u;
-        failed = __syncthreads_or(!ok) != 0;  // the shared tiles are free again once the MMAs are done
+        if (__syncthreads_or(!ok)) {  // timed out: drain the MMAs in flight (bounded), then leave
+            mbar_wait(bar, phase);
+            failed = true;
+            break;
+        }
+        phase ^= 1u;  // the shared tiles are free again once the MMAs are done
     }
     if (!failed && kb < ke) {
         // Epilogue: 32 accumulator columns at a time go through shared memory (the operand
@@ -406,7 +424,7 @@ __device__ __forceinline__ void stage_weights(uint32_t tile, const __half* __res
 __global__ void __launch_bounds__(128) predict_kernel(const uint4* __restrict__ st, uint32_t count,
                                                       const __half* __restrict__ w1h, const __half* __restrict__ w2h,
                                                       const float* __restrict__ params, float* __restrict__ out,
-                                                      unsigned* __restrict__ err) {
+                                                      uint32_t wait_limit, unsigned* __restrict__ err) {
     extern __shared__ unsigned char smem_raw[];
     const uint32_t raw = (uint32_t)__cvta_generic_to_shared(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;  // swizzle atoms need 1024-byte alignment
@@ -471,10 +489,13 @@ __global__ void __launch_bounds__(128) predict_kernel(const uint4* __restrict__ 
                     umma_f16(tmem, sw128_desc(xs + kstep_offset(k)), sw128_desc(wt + kstep_offset(k)), k > 0 ? 1u : 0u);
                 umma_commit(bar);
             }
-            const bool ok = mbar_wait(bar, phase);
+            const bool ok = wait_limit ? mbar_wait(bar, phase, wait_limit, true) : mbar_wait(bar, phase);
+            if (__syncthreads_or(!ok)) {  // timed out: drain the MMAs in flight (bounded), then leave
+                mbar_wait(bar, phase);
+                failed = true;
+                break;
+            }
             phase ^= 1u;
-            failed = __syncthreads_or(!ok) != 0;
-            if (failed) break;
             tc_fence_after();
             const float* bias = vec + layer * kH;
             for (uint32_t c = 0; c < (uint32_t)kH; c += 16) {
@@ -759,6 +780,11 @@ int nqb_model_features(const nqb_state* states, uint64_t count, float* out) {
 }
 
 int nqb_model_predict(const nqb_model* m, const nqb_state* states, uint64_t count, float* out) {
+    return nqb_model_predict_ex(m, states, count, out, 0);
+}
+
+int nqb_model_predict_ex(const nqb_model* m, const nqb_state* states, uint64_t count, float* out,
+                         uint32_t wait_limit) {
     if (!m || (count && (!states || !out))) return NQB_E_INVALID;
     if (count == 0) return NQB_OK;
     if (count > 0xFFFFFFFFull) return NQB_E_RANGE;
@@ -769,7 +795,7 @@ int nqb_model_predict(const nqb_model* m, const nqb_state* states, uint64_t coun
     int st = d_st.alloc(count);
     if (!st) st = d_out.alloc(count);
     if (!st) st = cuda_status(cudaMemcpyAsync(d_st.p, states, count * sizeof(nqb_state), cudaMemcpyHostToDevice, cs.s));
-    if (!st) st = nqb::model_predict_device(m, d_st.p, (uint32_t)count, d_out.p, cs.s);
+    if (!st) st = nqb::model_predict_device(m, d_st.p, (uint32_t)count, d_out.p, cs.s, wait_limit);
     if (!st) st = cuda_status(cudaMemcpyAsync(out, d_out.p, count * sizeof(float), cudaMemcpyDeviceToHost, cs.s));
     if (!st) st = cuda_status(cudaStreamSynchronize(cs.s));
     return st;
@@ -868,8 +894,9 @@ int nqb_model_train(nqb_model* m, const nqb_state* states, const float* targets,
 
 namespace nqb {
 
-int model_predict_device(const nqb_model* m, const nqb_state* d_states, uint32_t count, float* d_out, cudaStream_t s) {
-    if (count == 0) return NQB_OK;
+int model_predict_device(const nqb_model* m, const nqb_state* d_states, uint32_t count, float* d_out, cudaStream_t s,
+                         uint32_t wait_limit) {
+    if (count == 0) return NQB_OK;  // wait_limit 0: the default (suspending) bounded wait
     cudaError_t e = cudaFuncSetAttribute(predict_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPredictSmem);
     if (e != cudaSuccess) return cuda_status(e);
     int sms = 0;
@@ -883,7 +910,7 @@ int model_predict_device(const nqb_model* m, const nqb_state* d_states, uint32_t
     int st = cuda_status(cudaMemsetAsync(d_err, 0, sizeof(unsigned), s));
     if (!st) {
         predict_kernel<<<grid, kTileRows, kPredictSmem, s>>>(reinterpret_cast<const uint4*>(d_states), count, m->w1h,
-                                                             m->w2h, m->params, d_out, d_err);
+                                                             m->w2h, m->params, d_out, wait_limit, d_err);
         st = cuda_status(cudaGetLastError());
     }
     if (!st) st = cuda_status(cudaMemcpyAsync(&h_err, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));

@@ -103,8 +103,8 @@ void dev_free(void* p, cudaStream_t s);
 int cuda_status(cudaError_t e);
 
 // Learned cost model (mlp.cu): predicted log2(1 + nodes) of `count` device states.
-int model_predict_device(const nqb_model* m, const nqb_state* d_states, uint32_t count, float* d_out,
-                         cudaStream_t s);
+int model_predict_device(const nqb_model* m, const nqb_state* d_states, uint32_t count, float* d_out, cudaStream_t s,
+                         uint32_t wait_limit = 0);
 int model_device(const nqb_model* m);
 
 }  // namespace nqb

@@ -413,6 +413,13 @@ int nqb_model_set_params(nqb_model* model, const float* params /* NQB_MODEL_PARA
 int nqb_model_features(const nqb_state* states, uint64_t count, float* features);
 /* Predicted log2(1 + nodes) per state (fused tensor-core inference kernel). */
 int nqb_model_predict(const nqb_model* model, const nqb_state* states, uint64_t count, float* log2_nodes);
+/* Same, with an explicit bound on the wait for each tensor-core product: `wait_limit`
+ * non-blocking probes of its completion barrier (0 = the library's default bounded wait).
+ * A wait that runs out drains the products in flight, frees the block's tensor memory and
+ * makes the call return NQB_E_STALL with `log2_nodes` undefined; the model and the device
+ * stay usable.  A bound of 1 forces that path (tests). */
+int nqb_model_predict_ex(const nqb_model* model, const nqb_state* states, uint64_t count, float* log2_nodes,
+                         uint32_t wait_limit);
 /* One forward and backward pass over all `count` rows (count <= 2^20): mean squared
  * error and its gradient (NQB_MODEL_PARAMS floats), without updating the weights. */
 int nqb_model_loss_grad(nqb_model* model, const nqb_state* states, const float* targets, uint64_t count,

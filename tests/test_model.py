@@ -152,3 +152,17 @@ def test_predict_many_tiles(nqb, model):
     want, _ = mlp_ref.forward(model.get_params().astype(np.float64), mlp_ref.features(boards))
     assert np.max(np.abs(y - want)) < 2e-3 * max(1.0, np.max(np.abs(want)))
     assert np.array_equal(model.predict(boards[:1]), y[:1])  # a single, partial tile
+
+
+@pytest.mark.gpu
+def test_predict_wait_timeout_reports_stall_and_recovers(nqb, model):
+    """Failure detection without a fault: a one-iteration bound on the tensor-core completion
+    wait runs out, the kernel drains its products in flight, frees its tensor memory and the
+    call returns E_STALL; the next calls on the same model and device are exact again."""
+    boards = nqb.sample_boards(91, 50_000, 10, 20, 2, 6)
+    want = model.predict(boards)
+    with pytest.raises(nqb.NQBError) as e:
+        model.predict(boards, wait_limit=1)
+    assert e.value.status == nqb.E_STALL
+    assert np.array_equal(model.predict(boards), want)
+    assert nqb.count(14, 4, form=1, model=model) == 365596
