@@ -239,7 +239,7 @@ int nqb_read_state_file(const char* path, int header, unsigned expect_n, nqb_sta
  * :397-406; deffinitions.cuh:57,61): the lock row the reference picks for a requested
  * pool size `how_many`.  Hard limit = (uint64)(how_many * 1.2); the first row tried is
  * floor(log(how_many) / log(n)), at most n - 1 (NQB_E_INVALID when it is 0, i.e.
- * how_many < n).  Rows are tried downward while a row's pool is no smaller than the
+ * how_many < n).  Ever deeper rows are tried while a row's pool is no smaller than the
  * previous one, the row is at most n and the pool is within the hard limit; the answer
  * is the row tried before the last.  NQB_E_RANGE when the first row already exceeds the
  * limit.  If one row-0 column's pool reaches the limit the search ends there with the
@@ -268,7 +268,8 @@ int nqb_pool_for_target(unsigned n, uint64_t how_many, nqb_target* target);
  * count's work, in pool order); on it every candidate runs twice and the faster time
  * counts.  Candidates: both forms x block sizes 64, 128, 256, and with opts->model the
  * batched form's split factors 1, 4, 16.  All candidates of a depth must agree on the
- * sample's count (else NQB_E_DEVICE).  The fastest is reported with every candidate tried.
+ * sample's count (else NQB_E_DEVICE).  The fastest is reported with the candidates tried
+ * (the first 64 of them listed).
  */
 typedef struct nqb_tune_entry {
     unsigned depth;
