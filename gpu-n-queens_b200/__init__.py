@@ -15,7 +15,9 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libnqb.so")
+# NQB_LIBRARY selects another build of the same C ABI, e.g. the bounds-checked
+# libnqb_checked.so (`make -C gpu-n-queens_b200 checked`)
+LIB_PATH = os.environ.get("NQB_LIBRARY") or os.path.join(HERE, "libnqb.so")
 INCLUDE_DIR = os.path.join(os.path.dirname(HERE), "include")
 
 STATE_DTYPE = np.dtype([("cols", "<u4"), ("ldiag", "<u4"), ("rdiag", "<u4"),

@@ -58,12 +58,14 @@ __global__ void __launch_bounds__(BLOCK) batched_search_kernel(const BatchArgs a
     const uint32_t lt_mask = (1u << lane) - 1u;
     const uint32_t base0 = (uint32_t)__cvta_generic_to_shared(stack) + tid * 16;
 
+    const uint32_t top = base0 + a.stack_depth * kStride;  // the lane's last slot
     uint32_t base = base0;
     write_sentinel(base0);
     Lane s;
     lane_park(s, base);
     s.sols = 0;
     s.nodes = 0;
+    s.err = 0;
     uint32_t weight = 0, item = kNoItem;
     unsigned long long piece_sols = 0, piece_nodes = 0;  // folded lane counters of the current piece
     unsigned long long total = 0, total_nodes = 0;
@@ -155,16 +157,18 @@ __global__ void __launch_bounds__(BLOCK) batched_search_kernel(const BatchArgs a
             epoch = kEpoch;
         }
 #pragma unroll
-        for (int u = 0; u < kUnroll; ++u) search_step<kStride>(s, base);
+        for (int u = 0; u < kUnroll; ++u) search_step<kStride>(s, base, top);
     }
 
     total = warp_sum_u64(total);
     total_nodes = warp_sum_u64(total_nodes);
     const unsigned any_bad = __any_sync(kFull, bad);
+    const unsigned any_bound = __any_sync(kFull, s.err != 0);  // checked builds only
     if (lane == 0) {
         if (total) atomicAdd(a.out + 0, total);
         if (total_nodes) atomicAdd(a.out + 1, total_nodes);
         if (any_bad) atomicOr(a.out + 3, 1ull);
+        if (any_bound) atomicOr(a.out + 3, 2ull);
     }
 }
 

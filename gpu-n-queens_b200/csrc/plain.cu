@@ -21,7 +21,8 @@ constexpr int kUnroll = 16;
 constexpr uint32_t kEpoch = 1u << 27;  // votes between folds: kUnroll x kEpoch < 2^32
 
 // Error flags written to out[3].
-constexpr unsigned long long kErrStack = 1ull;  // a state needed a deeper stack than provided
+constexpr unsigned kErrStack = 1u;  // a state needed a deeper stack than provided
+constexpr unsigned kErrBound = 2u;  // checked builds: a push would have passed a lane's last slot
 
 // per_state (optional): weight x completions of each state, for per-board results.
 // UNIT: also count placements made by unit-row propagation (the reference's split of
@@ -36,12 +37,14 @@ __global__ void __launch_bounds__(BLOCK) plain_search_kernel(const uint4* __rest
     const uint32_t tid = threadIdx.x;
     const uint32_t gi = blockIdx.x * BLOCK + tid;
     const uint32_t base = (uint32_t)__cvta_generic_to_shared(stack) + tid * 16;
+    const uint32_t top = base + stack_depth * kStride;  // the lane's last slot
     write_sentinel(base);
 
     Lane s;
     lane_park(s, base);
     s.sols = 0;
     s.nodes = 0;
+    s.err = 0;
     uint32_t weight = 0;
     bool bad = false;
     if (gi < count) {
@@ -70,7 +73,7 @@ __global__ void __launch_bounds__(BLOCK) plain_search_kernel(const uint4* __rest
                 unit += (!first && s.avail != 0 && (s.avail & (s.avail - 1u)) == 0);
                 first = false;
             }
-            search_step<kStride>(s, base);
+            search_step<kStride>(s, base, top);
         }
     }
     sols += s.sols;
@@ -82,7 +85,7 @@ __global__ void __launch_bounds__(BLOCK) plain_search_kernel(const uint4* __rest
     c = warp_sum_u64(c);
     nodes = warp_sum_u64(nodes);
     if (UNIT) un = warp_sum_u64(un);
-    const unsigned any_bad = __any_sync(kFull, bad);
+    const unsigned flags = (__any_sync(kFull, bad) ? kErrStack : 0u) | (__any_sync(kFull, s.err != 0) ? kErrBound : 0u);
 
     __syncthreads();  // the stack area is reused for the block reduction
     unsigned long long* red = reinterpret_cast<unsigned long long*>(stack);
@@ -92,23 +95,22 @@ __global__ void __launch_bounds__(BLOCK) plain_search_kernel(const uint4* __rest
         red[warp] = c;
         red[kWarps + warp] = nodes;
         red[2 * kWarps + warp] = un;
-        red[3 * kWarps + warp] = any_bad;
+        red[3 * kWarps + warp] = flags;
     }
     __syncthreads();
     if (warp == 0) {
         c = lane < kWarps ? red[lane] : 0;
         nodes = lane < kWarps ? red[kWarps + lane] : 0;
         un = lane < kWarps ? red[2 * kWarps + lane] : 0;
-        unsigned long long of = lane < kWarps ? red[3 * kWarps + lane] : 0;
+        const unsigned of = warp_or(lane < kWarps ? (unsigned)red[3 * kWarps + lane] : 0u);
         c = warp_sum_u64(c);
         nodes = warp_sum_u64(nodes);
         un = warp_sum_u64(un);
-        of = warp_sum_u64(of);
         if (lane == 0) {
             if (c) atomicAdd(out + 0, c);
             atomicAdd(out + 1, nodes);
             if (UNIT && un) atomicAdd(out + 2, un);
-            if (of) atomicOr(out + 3, kErrStack);
+            if (of) atomicOr(out + 3, (unsigned long long)of);
         }
     }
 }

@@ -27,7 +27,9 @@
 // Stack bound: a row is pushed only while another free column remains, and pushed
 // rows are strictly deeper towards the top, so a search from a state with f free
 // columns holds at most f - 1 entries.  Kernels check that bound once per item, so the
-// step itself carries no bounds check.
+// step itself carries no bounds check.  Built with NQB_CHECKS (the checked library), every
+// push is also compared with `top`, the lane's last slot: a push past it is dropped and
+// sets bit 0 of the lane's `err`, which the kernels report as a device error.
 #pragma once
 
 #include <cstdint>
@@ -42,6 +44,7 @@ struct Lane {
     uint32_t sp;     // shared byte address of the top entry; == base when the stack is empty
     uint32_t sols;   // solutions since the last fold
     uint32_t nodes;  // placements since the last fold
+    uint32_t err;    // NQB_CHECKS builds: bit 0 = a push would have passed the lane's last slot
 };
 
 __device__ __forceinline__ uint4 lds128(uint32_t addr) {
@@ -62,9 +65,12 @@ __device__ __forceinline__ void write_sentinel(uint32_t addr) {
     sts128(addr, make_uint4(0u, kSentinelNc, kSentinelL, 0u));
 }
 
-// One step; STRIDE is the byte distance between a lane's stack entries (BLOCK x 16).
+// One step; STRIDE is the byte distance between a lane's stack entries (BLOCK x 16);
+// `top` is the byte address of the lane's last stack slot (checked builds only).
 template <int STRIDE>
-__device__ __forceinline__ void search_step(Lane& s, uint32_t base) {
+__device__ __forceinline__ void search_step(Lane& s, uint32_t base, uint32_t top) {
+#ifndef NQB_CHECKS
+    (void)top;
     asm volatile(
         "{\n\t.reg .pred p, q, t;\n\t.reg .u32 b, nb;\n\t"
         "setp.eq.u32 p, %0, 0;\n\t"                        // no candidate left: pop
@@ -92,6 +98,40 @@ __device__ __forceinline__ void search_step(Lane& s, uint32_t base) {
         : "+r"(s.avail), "+r"(s.nc), "+r"(s.l), "+r"(s.r), "+r"(s.sp), "+r"(s.nodes), "+r"(s.sols)
         : "r"(base), "n"(STRIDE)
         : "memory");
+#else
+    asm volatile(
+        "{\n\t.reg .pred p, q, t, ov, ok;\n\t.reg .u32 b, nb, nsp;\n\t"
+        "setp.eq.u32 p, %0, 0;\n\t"
+        "@p ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n\t"
+        "setp.ne.and.u32 q, %4, %8, p;\n\t"
+        "@q sub.u32 %4, %4, %9;\n\t"
+        "neg.s32 nb, %0;\n\t"
+        "and.b32 b, %0, nb;\n\t"
+        "sub.u32 %0, %0, b;\n\t"
+        "setp.ne.u32 t, %0, 0;\n\t"
+        "add.u32 nsp, %4, %9;\n\t"                         // the push's slot must not pass top
+        "setp.gt.u32 ov, nsp, %10;\n\t"
+        "and.pred ok, t, !ov;\n\t"
+        "@ok mov.u32 %4, nsp;\n\t"
+        "@ok st.shared.v4.u32 [%4], {%0, %1, %2, %3};\n\t"
+        "and.pred ov, t, ov;\n\t"
+        "@ov or.b32 %7, %7, 1;\n\t"
+        "sub.u32 %1, %1, b;\n\t"
+        "add.u32 %2, %2, b;\n\t"
+        "shl.b32 %2, %2, 1;\n\t"
+        "add.u32 %3, %3, b;\n\t"
+        "shr.u32 %3, %3, 1;\n\t"
+        "or.b32 nb, %2, %3;\n\t"
+        "not.b32 nb, nb;\n\t"
+        "and.b32 %0, %1, nb;\n\t"
+        "setp.ne.u32 t, b, 0;\n\t"
+        "@t add.u32 %5, %5, 1;\n\t"
+        "setp.eq.u32 t, %1, 0;\n\t"
+        "@t add.u32 %6, %6, 1;\n\t}"
+        : "+r"(s.avail), "+r"(s.nc), "+r"(s.l), "+r"(s.r), "+r"(s.sp), "+r"(s.nodes), "+r"(s.sols), "+r"(s.err)
+        : "r"(base), "n"(STRIDE), "r"(top)
+        : "memory");
+#endif
 }
 
 // Loads a state {cols, ldiag, rdiag, meta} into a lane with an empty stack.  Returns
@@ -116,6 +156,12 @@ __device__ __forceinline__ void lane_park(Lane& s, uint32_t base) {
     s.l = kSentinelL;
     s.r = 0;
     s.sp = base;
+}
+
+__device__ __forceinline__ unsigned warp_or(unsigned v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v |= __shfl_down_sync(0xFFFFFFFFu, v, o);
+    return v;
 }
 
 __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
