@@ -29,6 +29,20 @@
 
 namespace {
 
+// A library-allocated array (released with nqb_free), used in place.
+template <class T>
+struct LibArray {
+    T* p = nullptr;
+    uint64_t n = 0;
+    LibArray() = default;
+    LibArray(const LibArray&) = delete;
+    LibArray& operator=(const LibArray&) = delete;
+    ~LibArray() { nqb_free(p); }
+    T* data() const { return p; }
+    uint64_t size() const { return n; }
+    T& operator[](uint64_t i) const { return p[i]; }
+};
+
 struct Opt {
     char key;
     const char* shorts;  // accepted short letters
@@ -74,8 +88,8 @@ std::string with_commas(uint64_t v) {
 // shuffle_states (NQ_solver.cu:40-55): for i in [0, len - 2) swap i with
 // ((r mod len) + i) mod len, r = four rand() values as the 16-bit lanes of a uint64.
 // Below 3 states nothing moves (the reference's bound len - 2 wraps there).
-template <class T>
-void shuffle(std::vector<T>& v) {
+template <class A>
+void shuffle(A& v) {
     const uint64_t len = v.size();
     if (len < 3) return;
     for (uint64_t i = 0; i < len - 2; ++i) {
@@ -99,7 +113,7 @@ int nqb_fail(const char* what, int status) {
 
 // write_gen_states_to_file (NQ_solver.cu:57-108): one file, or `chunks` files of
 // ceil(count / chunks) states, one fewer after the first count % chunks files.
-int write_states(const std::vector<nqb_placement>& pl, unsigned n, unsigned lock, int chunks, const char* out) {
+int write_states(const LibArray<nqb_placement>& pl, unsigned n, unsigned lock, int chunks, const char* out) {
     const uint64_t cnt = pl.size();
     if (!chunks) {
         std::printf("Writing generated states to file...");
@@ -261,7 +275,7 @@ int print_target(unsigned n, uint64_t how_many, nqb_target* t) {
     return s;
 }
 
-int solve_and_print(const std::vector<nqb_state>& states, unsigned n, const Args& a) {
+int solve_and_print(const nqb_state* states, uint64_t count, unsigned n, const Args& a) {
     nqb_opts o;
     nqb_default_opts(&o);
     o.form = a.form;
@@ -278,8 +292,7 @@ int solve_and_print(const std::vector<nqb_state>& states, unsigned n, const Args
     std::printf("Solving...\n");
     uint64_t total = 0;
     nqb_stats st;
-    const int s = nqb_solve_states_multi(states.data(), states.size(), devs.data(), (unsigned)devs.size(), &o, &total,
-                                         &st);
+    const int s = nqb_solve_states_multi(states, count, devs.data(), (unsigned)devs.size(), &o, &total, &st);
     if (s) return nqb_fail("Solving failed", s);
     std::printf("solution_count(%u) = %" PRIu64 " (%s)\n", n, total, with_commas(total).c_str());
     std::printf("\t%" PRIu64 " states on %zu device(s), %" PRIu64 " nodes, kernel %.3f ms, wall %.3f ms\n", st.states,
@@ -287,7 +300,7 @@ int solve_and_print(const std::vector<nqb_state>& states, unsigned n, const Args
     return EXIT_SUCCESS;
 }
 
-std::vector<nqb_state> to_states(const std::vector<nqb_placement>& pl, int* status) {
+std::vector<nqb_state> to_states(const LibArray<nqb_placement>& pl, int* status) {
     std::vector<nqb_state> st(pl.size());
     *status = nqb_states_from_placements(pl.data(), pl.size(), 1, st.data());
     return st;
@@ -318,12 +331,9 @@ int main(int argc, char** argv) {
             if (s) return nqb_fail("State generation failed", s);
             lock = t.lock_row;
         }
-        nqb_placement* p = nullptr;
-        uint64_t cnt = 0;
-        const int s = nqb_generate_pool_placements(a.n, lock == 1 ? 2 : lock, &p, &cnt);  // lock row 1: 2-row states
+        LibArray<nqb_placement> pl;
+        const int s = nqb_generate_pool_placements(a.n, lock == 1 ? 2 : lock, &pl.p, &pl.n);  // lock row 1: 2-row states
         if (s) return nqb_fail("State generation failed", s);
-        std::vector<nqb_placement> pl(p, p + cnt);
-        nqb_free(p);
         if (a.shuffle) shuffle(pl);
         const int w = write_states(pl, a.n, lock, a.split, a.gen_file);
         if (w) return w;
@@ -335,24 +345,23 @@ int main(int argc, char** argv) {
         if (a.try_count) std::printf("Ignoring solving state count flag -- This is not applicable here.\n");
         std::printf("Loading states from file...\n");
         nqb_state_file info;
-        nqb_placement* p = nullptr;
-        int s = nqb_read_state_file(a.in_file, 1, a.n_given ? a.n : 0, &info, &p);
+        LibArray<nqb_placement> pl;
+        int s = nqb_read_state_file(a.in_file, 1, a.n_given ? a.n : 0, &info, &pl.p);
         if (s) return nqb_fail("Failed to read states from file", s);
-        std::vector<nqb_placement> pl(p, p + info.count);
-        nqb_free(p);
+        pl.n = info.count;
         std::printf("Loaded %" PRIu64 " states\n", info.count);
         if (a.shuffle) {
             std::printf("Shuffling loaded states...\n");
             shuffle(pl);
         }
         bool other_rows = false;
-        for (const nqb_placement& q : pl) other_rows |= q.row != info.locked_row;
+        for (uint64_t i = 0; i < pl.size(); ++i) other_rows |= pl[i].row != info.locked_row;
         if (other_rows)
             std::printf("Note: states start below the file's locked row %u; each is solved from its own row "
                         "(the reference's kernel would also search rows above them).\n", info.locked_row);
         const std::vector<nqb_state> st = to_states(pl, &s);
         if (s) return nqb_fail("Invalid states in file", s);
-        return solve_and_print(st, info.n, a);
+        return solve_and_print(st.data(), st.size(), info.n, a);
     }
 
     // count-target pool, solved
@@ -363,12 +372,9 @@ int main(int argc, char** argv) {
     nqb_target t;
     int s = print_target(a.n, (uint64_t)a.try_count, &t);
     if (s) return nqb_fail("Failed to generate states", s);
-    nqb_state* p = nullptr;
-    uint64_t cnt = 0;
-    s = nqb_generate_pool(a.n, t.pool_depth, &p, &cnt);
+    LibArray<nqb_state> st;
+    s = nqb_generate_pool(a.n, t.pool_depth, &st.p, &st.n);
     if (s) return nqb_fail("Failed to generate states", s);
-    std::vector<nqb_state> st(p, p + cnt);
-    nqb_free(p);
-    std::printf("%" PRIu64 " states generated.\n", cnt);
-    return solve_and_print(st, a.n, a);
+    std::printf("%" PRIu64 " states generated.\n", st.size());
+    return solve_and_print(st.data(), st.size(), a.n, a);
 }
