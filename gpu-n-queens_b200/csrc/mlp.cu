@@ -12,7 +12,7 @@
 //   dy = 2 (y - t)      dZ2 = dy w3^T * gelu'(Z2 + b2)      dH1 = dZ2 W2^T
 //   dZ1 = dH1 * gelu'(Z1 + b1)
 //   dW2 = H1^T dZ2 / B  dW1 = X^T dZ1 / B  dw3 = H2^T dy / B  (bias grads: column sums / B)
-// All GEMMs go through one tiled kernel with arbitrary operand strides (gemm_f16).
+// All GEMMs go through one tcgen05 kernel with arbitrary operand strides (gemm_tc).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
