@@ -14,7 +14,7 @@ on the host and copied over, `host_pool`) is timed once beside it.  Prints one J
 reference's sources) on bounded stride samples of the same pool with every host core,
 and, for comparison, the reference CUDA build on the same GPU.
 
-Multi-GPU: the north star is one GPU, so N > 1 runs N independent replicas (weak
+Multi-GPU: the count runs on one GPU, so N > 1 runs N independent replicas (weak
 scaling, no collective on the data path); the step time is the max over ranks.
 """
 import argparse
@@ -357,7 +357,7 @@ def run_nqb(args):
 
 
 def run_extras(nqb, dev, args):
-    """The learned model and the other north-star workloads, beside the headline (not timed
+    """The learned model and the other workloads of the project, beside the headline (not timed
     as the bench value): the cost model trained on 1M seeded N=18 prefixes (depth 4..8) with
     node counts recorded by the solver; the 65,536 uneven partial boards solved through an
     autotuned learned plan (CUDA graph) against the batched form without a model; the N=19
