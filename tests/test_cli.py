@@ -131,3 +131,16 @@ def test_solve_chunks_sum_to_count():
 def test_count_target_solve(args, n):
     got_n, c = solution(run(*args))
     assert got_n == n and c == KAT[n]
+
+
+@pytest.mark.parametrize("lock,states", [(2, 2), (3, 1)])
+def test_shuffle_of_tiny_pools_keeps_order(lock, states, tmp_path, nqsf):
+    """The reference's shuffle loops over [0, len - 2), which wraps below two states (it
+    would run off the buffer); here fewer than three states keep their order, and the file
+    equals the unshuffled one."""
+    a, b = tmp_path / "m.nqsf", tmp_path / "p.nqsf"
+    assert run("-n", 4, "-R", lock, "-m", "-w", a).returncode == 0
+    assert run("-n", 4, "-R", lock, "-w", b).returncode == 0
+    assert a.read_bytes() == b.read_bytes()
+    assert nqsf.read_bytes(a.read_bytes())[4] == states
+    assert nqsf.shuffle_perm(states) == list(range(states))
