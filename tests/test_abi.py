@@ -86,3 +86,33 @@ def test_struct_layouts_match_header(nqb, tmp_path):
             assert got[(cname, f[0])] == getattr(cls, f[0]).offset, (cname, f[0])
     assert got[("nqb_placement", "size")] == nqb.PLACEMENT_DTYPE.itemsize == 32
     assert got[("nqb_state", "size")] == nqb.STATE_DTYPE.itemsize == 16
+
+
+def test_new_entry_points_reject_bad_arguments_without_a_device(nqb):
+    """Argument checks come before any device work, so they answer on a machine without a
+    GPU as on a B200."""
+    L = nqb.lib()
+    u64 = ctypes.c_uint64()
+    vp = ctypes.c_void_p()
+    r = nqb.TuneResult()
+    ds = (ctypes.c_uint * 1)(17)
+    assert L.nqb_tune_count(17, ds, 1, None, 64, ctypes.byref(r)) == nqb.E_INVALID      # depth == n
+    ds[0] = 5
+    assert L.nqb_tune_count(17, ds, 1, None, 0, ctypes.byref(r)) == nqb.E_INVALID       # sample_div 0
+    assert L.nqb_tune_count(17, None, 1, None, 64, ctypes.byref(r)) == nqb.E_INVALID
+    assert L.nqb_tune_count(3, ds, 1, None, 64, ctypes.byref(r)) == nqb.E_INVALID       # n below 4
+    devs = (ctypes.c_int * 1)(0)
+    assert L.nqb_solve_states_multi(None, 0, None, 1, None, ctypes.byref(u64), None) == nqb.E_INVALID
+    assert L.nqb_solve_states_multi(None, 0, devs, 0, None, ctypes.byref(u64), None) == nqb.E_INVALID
+    assert L.nqb_solve_states_multi(None, 5, devs, 1, None, ctypes.byref(u64), None) == nqb.E_INVALID
+    for n, d in [(3, 1), (32, 5), (10, 0), (10, 10)]:
+        assert L.nqb_generate_pool_device(n, d, ctypes.byref(vp), ctypes.byref(u64), None) == nqb.E_INVALID
+    assert L.nqb_measure_int32_peak(0, None, None) == nqb.E_INVALID
+    assert L.nqb_trim_device_memory(-1) == nqb.E_NODEVICE
+    assert L.nqb_trim_device_memory(64) == nqb.E_NODEVICE
+    assert L.nqb_model_predict_ex(None, None, 0, None, 0) == nqb.E_INVALID
+    assert L.nqb_device_count(None) == nqb.E_INVALID
+    t = nqb.Target()
+    assert L.nqb_pool_for_target(8, 0, ctypes.byref(t)) == nqb.E_INVALID
+    assert L.nqb_pool_for_target(40, 100, ctypes.byref(t)) == nqb.E_INVALID
+    assert L.nqb_pool_for_target(8, 100, None) == nqb.E_INVALID
