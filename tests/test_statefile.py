@@ -230,3 +230,19 @@ def test_state_file_errors(nqb, tmp_path):
         with pytest.raises(nqb.NQBError) as e:
             nqb.pool_for_target(8, h)
         assert e.value.status == nqb.E_INVALID
+
+
+def test_row_zero_states_round_trip(nqb, nqsf, tmp_path):
+    """Empty boards (row 0) take no column bytes in a file; they still count toward the
+    total, in a segment of their own, and read back as boards with no queen."""
+    pl = np.zeros(3, dtype=nqb.PLACEMENT_DTYPE)
+    pl["n"], pl["row"], pl["col"] = 9, 0, 0xFF
+    mix = np.concatenate([pl, nqb.generate_pool_placements(9, 2)[:4]])
+    out = str(tmp_path / "r0.nqsf")
+    nqb.write_state_file(out, mix, 9, 0)
+    data = open(out, "rb").read()
+    assert data == nqsf.write_bytes(9, 0, [(0, [])] * 3 + [(2, list(c[:2])) for c in mix[3:]["col"]])
+    info, back = nqb.read_state_file(out)
+    assert info["count"] == 7 and np.array_equal(back, mix)
+    st = nqb.states_from_placements(back[:3])
+    assert np.all(st["cols"] == 0) and np.all(st["weight"] == 1) and np.all(st["row"] == 0)
