@@ -116,3 +116,40 @@ def test_new_entry_points_reject_bad_arguments_without_a_device(nqb):
     assert L.nqb_pool_for_target(8, 0, ctypes.byref(t)) == nqb.E_INVALID
     assert L.nqb_pool_for_target(40, 100, ctypes.byref(t)) == nqb.E_INVALID
     assert L.nqb_pool_for_target(8, 100, None) == nqb.E_INVALID
+
+
+def test_c_program_links_and_runs(tmp_path):
+    """A C program, as the reference's own code would call the library: compiled against
+    include/nqb.h, linked with -lnqb, it sizes a pool by count target, writes it as a state
+    file, reads it back and rebuilds the search states (the host-side entry points)."""
+    from conftest import PKG_DIR, ROOT
+    src = tmp_path / "use_nqb.c"
+    src.write_text(r'''
+#include <stdio.h>
+#include <string.h>
+#include "nqb.h"
+int main(int argc, char** argv) {
+    nqb_target t;
+    if (nqb_pool_for_target(10, 1334, &t) != NQB_OK) return 1;
+    nqb_placement* pl = NULL; uint64_t cnt = 0;
+    if (nqb_generate_pool_placements(10, t.pool_depth, &pl, &cnt) != NQB_OK || cnt != t.count) return 2;
+    if (nqb_write_state_file(argv[1], pl, cnt, 10, t.lock_row, 1) != NQB_OK) return 3;
+    nqb_state_file info; nqb_placement* back = NULL;
+    if (nqb_read_state_file(argv[1], 1, 10, &info, &back) != NQB_OK || info.count != cnt) return 4;
+    if (memcmp(pl, back, cnt * sizeof(nqb_placement)) != 0) return 5;
+    nqb_state st[700], pool[700]; uint64_t pc = 0;
+    if (cnt > 700 || nqb_states_from_placements(back, cnt, 1, st) != NQB_OK) return 6;
+    if (nqb_generate_pool_into(10, t.pool_depth, pool, 700, &pc) != NQB_OK || pc != cnt) return 7;
+    if (memcmp(st, pool, cnt * sizeof(nqb_state)) != 0) return 8;
+    printf("lock %u states %llu\n", t.lock_row, (unsigned long long)cnt);
+    nqb_free(pl); nqb_free(back);
+    return strcmp(nqb_strerror(NQB_E_FORMAT), "unknown status") == 0 ? 9 : 0;
+}
+''')
+    exe = tmp_path / "use_nqb"
+    subprocess.run(["gcc", "-std=c11", "-O1", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                    "-L", PKG_DIR, "-lnqb", f"-Wl,-rpath,{PKG_DIR}"], check=True)
+    p = subprocess.run([str(exe), str(tmp_path / "pool.nqsf")], capture_output=True, text=True)
+    assert p.returncode == 0 and p.stdout.strip() == "lock 4 states 697", (p.returncode, p.stdout, p.stderr)
+    golden = os.path.join(ROOT, "tests", "golden", "nqsf", "g_n10_1334.nqsf")
+    assert (tmp_path / "pool.nqsf").read_bytes() == open(golden, "rb").read()  # the reference CLI's -g 1334
