@@ -2,6 +2,7 @@
 // rules of the reference's CLI path (nq_utils.cu:127-259, n_queens.cu:128-219 and :397-406),
 // over the same pool as the search (pool.cpp).
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -13,6 +14,10 @@ namespace nqb {
 namespace {
 
 constexpr unsigned kMaxRow = sizeof(((nqb_placement*)nullptr)->col);  // 30
+// Largest number of row-0 boards one file may hold (their segment has no bytes to bound it).
+constexpr uint64_t kMaxRow0Boards = 1ull << 32;
+// Largest number of boards whose placements fit one allocation.
+constexpr uint64_t kMaxPlacements = SIZE_MAX / sizeof(nqb_placement);
 
 bool placement_ok(const nqb_placement& p) {
     if (p.n < NQB_MIN_N || p.n > NQB_MAX_N || p.row >= p.n || p.row > kMaxRow) return false;
@@ -184,16 +189,21 @@ int nqb_read_state_file(const char* path, int header, unsigned expect_n, nqb_sta
         if (!get(f, &cnt)) return fail(NQB_E_FORMAT);
         if (r >= n8 || r > kMaxRow || cnt > total - filled) return fail(NQB_E_FORMAT);
         const uint64_t left = (uint64_t)(fsize - std::ftell(f));
-        if (r && cnt > left / r) return fail(NQB_E_FORMAT);
-        if (filled + cnt > cap) {
-            cap = filled + cnt;
-            nqb_placement* q = static_cast<nqb_placement*>(std::realloc(p, (cap ? cap : 1) * sizeof(nqb_placement)));
-            if (!q) return fail(NQB_E_NOMEM);
-            p = q;
-        }
+        // A segment of row r > 0 carries r bytes a board, so the file size bounds its count;
+        // boards of row 0 carry none, so their count has a fixed bound instead.
+        if (r ? cnt > left / r : cnt > kMaxRow0Boards) return fail(NQB_E_FORMAT);
+        if (cnt > kMaxPlacements - filled) return fail(NQB_E_FORMAT);
         const uint64_t chunk = 1u << 16;  // states per read
         for (uint64_t done = 0; done < cnt;) {
             const uint64_t k = cnt - done < chunk ? cnt - done : chunk;
+            if (filled + done + k > cap) {  // grow as boards arrive, at most to the segment's end
+                uint64_t want = cap * 2 > filled + cnt ? filled + cnt : cap * 2;
+                if (want < filled + done + k) want = filled + done + k;
+                nqb_placement* q = static_cast<nqb_placement*>(std::realloc(p, want * sizeof(nqb_placement)));
+                if (!q) return fail(NQB_E_NOMEM);
+                p = q;
+                cap = want;
+            }
             cols.resize(k * r);
             if (r && std::fread(cols.data(), 1, k * r, f) != k * r) return fail(NQB_E_FORMAT);
             for (uint64_t j = 0; j < k; ++j) {

@@ -246,3 +246,25 @@ def test_row_zero_states_round_trip(nqb, nqsf, tmp_path):
     assert info["count"] == 7 and np.array_equal(back, mix)
     st = nqb.states_from_placements(back[:3])
     assert np.all(st["cols"] == 0) and np.all(st["weight"] == 1) and np.all(st["row"] == 0)
+
+
+def test_row_zero_segment_counts_are_bounded(nqb, tmp_path):
+    """A row-0 segment carries no column bytes, so the file size cannot bound its count: a
+    count whose placement array would not fit (or whose byte size wraps) is a format error,
+    not an allocation; a large but plausible count reads back as empty boards."""
+    import struct
+    good = golden_bytes("R_n8_l3.nqsf")
+    p = tmp_path / "z.nqsf"
+
+    def file_with(total, cnt):
+        return good[:12] + bytes([8, 0]) + struct.pack("<Q", total) + bytes([0]) + struct.pack("<Q", cnt)
+
+    for cnt in (2 ** 59 + 1, 2 ** 63, 2 ** 32 + 1):
+        p.write_bytes(file_with(cnt, cnt))
+        with pytest.raises(nqb.NQBError) as e:
+            nqb.read_state_file(str(p))
+        assert e.value.status == nqb.E_FORMAT, cnt
+    p.write_bytes(file_with(1 << 16, 1 << 16))
+    info, back = nqb.read_state_file(str(p))
+    assert info["count"] == 1 << 16 and len(back) == 1 << 16
+    assert np.all(back["row"] == 0) and np.all(back["n"] == 8)
