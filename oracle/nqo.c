@@ -7,7 +7,8 @@
  *
  * Parity pins: the reference's known-answer table (test.cu:18), its weighted pool
  * sizes (test.cu:88-104), and outputs of the reference's own host code built from
- * its sources by oracle/build_ref.sh (tests/golden/ holds the captured vectors).
+ * its sources by oracle/Makefile (`make -C oracle ref`; tests/golden/ holds the
+ * captured vectors).
  *
  * Reference state model restated here (n_queens.cuh:100-113, diagonals.cuh:8-34):
  *   diag bit (c + i) and anti bit (c + N - i) mark the queen at row i, column c;

@@ -1,9 +1,11 @@
 """Regenerates tests/golden/ref_vectors.json from the reference itself.
 
-Run in the build container (it reads the reference sources and runs oracle/_ref, the
-reference's own code built by `make -C oracle ref`):
+Run where the reference's sources are (it reads them and runs oracle/_ref, the
+reference's own code built by `make -C oracle ref REF_DIR=<reference checkout>`):
 
-    python tests/golden/make_golden.py [--quick]
+    python tests/golden/make_golden.py --reference <reference checkout> [--quick]
+
+(`--reference` may be left out when NQB_REFERENCE_DIR names the checkout.)
 
 Captured:
   kat_counts       the known-answer table of check_if_known_result (test.cu:17-24)
@@ -14,6 +16,7 @@ Captured:
   replays          ref_harness `replay`: the reference kernel loop replayed on the host
                    over the pool (or a stride sample of it): weighted count, nodes, unit
 """
+import argparse
 import json
 import os
 import re
@@ -23,7 +26,7 @@ from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF_SRC = os.environ.get("NQO_REF_DIR", "/root/reference")
+REF_SRC = None  # the reference checkout: --reference, else NQB_REFERENCE_DIR
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "N{n}", "ref_harness")
 
 POOLS = [(n, d) for n in range(8, 15) for d in range(1, n)] + [
@@ -52,7 +55,15 @@ def read_test_tables():
 
 
 def main():
-    quick = "--quick" in sys.argv
+    global REF_SRC
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--reference", default=os.environ.get("NQB_REFERENCE_DIR"),
+                    help="the reference checkout (default: $NQB_REFERENCE_DIR)")
+    ap.add_argument("--quick", action="store_true", help="keep the largest replays from the existing file")
+    args = ap.parse_args()
+    if not args.reference or not os.path.isfile(os.path.join(args.reference, "test.cu")):
+        ap.error("--reference (or NQB_REFERENCE_DIR) must name the reference checkout")
+    REF_SRC, quick = args.reference, args.quick
     kat, files = read_test_tables()
     with ThreadPoolExecutor(max_workers=os.cpu_count()) as ex:
         pools = list(ex.map(lambda nd: run(nd[0], "pool", nd[1]), POOLS))
