@@ -192,8 +192,10 @@ def run_nqb(args):
     states = len(pool)
     stack_depth = n - d - 1
     d_pool = torch.from_numpy(pool.view(np.uint8)).to(f"cuda:{dev}")
-    d_out = torch.zeros((max(args.steps, args.warmup), 4), dtype=torch.int64, device=f"cuda:{dev}")
-    d_head = torch.zeros(max(args.steps, args.warmup), dtype=torch.int32, device=f"cuda:{dev}")
+    slots = max(args.steps, args.warmup)
+    d_out = torch.zeros((slots, 4), dtype=torch.int64, device=f"cuda:{dev}")
+    # the batched launch's scratch (control words + steal ring), one zeroed buffer per step
+    d_scratch = torch.zeros((slots, nqb.BATCHED_SCRATCH_BYTES), dtype=torch.uint8, device=f"cuda:{dev}")
     stream = torch.cuda.current_stream(dev)
     sptr = stream.cuda_stream
     form = {"plain": nqb.FORM_PLAIN, "batched": nqb.FORM_BATCHED}[args.form]
@@ -207,20 +209,20 @@ def run_nqb(args):
             blocks[f] = min((t for t in tuning["tried"] if t["form"] == f and t["depth"] == d),
                             key=lambda t: t["ms"])["block_size"]
 
-    def launch(f, out_row, head_slot):
+    def launch(f, out_row, scratch):
         if f == nqb.FORM_PLAIN:
             nqb.plain_launch(d_pool.data_ptr(), states, out_row.data_ptr(), block_size=blocks[f],
                              stack_depth=stack_depth, stream=sptr)
         else:
-            nqb.batched_launch(d_pool.data_ptr(), states, head_slot.data_ptr(), out_row.data_ptr(),
-                               block_size=blocks[f], stack_depth=stack_depth, stream=sptr)
+            nqb.batched_launch_ex(d_pool.data_ptr(), states, scratch.data_ptr(), scratch.numel(),
+                                  out_row.data_ptr(), block_size=blocks[f], stack_depth=stack_depth, stream=sptr)
 
     def step(i):
-        launch(form, d_out[i], d_head[i:i + 1])
+        launch(form, d_out[i], d_scratch[i])
 
     # warm-up (untimed), also the correctness check
     d_out.zero_()
-    d_head.zero_()
+    d_scratch.zero_()
     for i in range(args.warmup):
         step(i)
     torch.cuda.synchronize(dev)
@@ -235,7 +237,7 @@ def run_nqb(args):
 
     # timed region: K full counts, pool resident in HBM (630 MB > L2 at n=21 d=7)
     d_out.zero_()
-    d_head.zero_()
+    d_scratch.zero_()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if world > 1:
         dist.barrier()
@@ -253,23 +255,37 @@ def run_nqb(args):
     ms_step = ms / args.steps
     value = replica_rate(nodes, world, ms_step / 1e3)
 
-    # the other form once on the same resident pool, for the plain-vs-batched comparison
-    forms = {args.form: {"ms": round(ms_step, 3), "nodes_per_s": round(nodes / (ms_step / 1e3), 1)}}
+    # the other form on the same resident pool, K steps, for the plain-vs-batched comparison
+    forms = {args.form: {"ms": round(ms_step, 3), "nodes_per_s": round(nodes / (ms_step / 1e3), 1),
+                         "steps": args.steps}}
     if not args.skip_other_form:
         other = "plain" if args.form == "batched" else "batched"
-        o_out = torch.zeros(4, dtype=torch.int64, device=f"cuda:{dev}")
-        o_head = torch.zeros(1, dtype=torch.int32, device=f"cuda:{dev}")
+        d_out.zero_()
+        d_scratch.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        launch({"plain": nqb.FORM_PLAIN, "batched": nqb.FORM_BATCHED}[other], o_out, o_head)
+        for i in range(args.steps):
+            launch({"plain": nqb.FORM_PLAIN, "batched": nqb.FORM_BATCHED}[other], d_out[i], d_scratch[i])
         e1.record(stream)
         torch.cuda.synchronize(dev)
-        o = o_out.cpu().numpy().astype(np.uint64)
-        assert int(o[0]) == count and int(o[1]) == nodes and int(o[3]) == 0
-        oms = e0.elapsed_time(e1)
-        forms[other] = {"ms": round(oms, 3), "nodes_per_s": round(nodes / (oms / 1e3), 1), "steps": 1}
+        o = d_out.cpu().numpy().astype(np.uint64)
+        assert all(int(o[i, 0]) == count and int(o[i, 1]) == nodes and int(o[i, 3]) == 0 for i in range(args.steps))
+        oms = e0.elapsed_time(e1) / args.steps
+        forms[other] = {"ms": round(oms, 3), "nodes_per_s": round(nodes / (oms / 1e3), 1), "steps": args.steps}
         if "plain" in forms and "batched" in forms:
             forms["batched_over_plain"] = round(forms["plain"]["ms"] / forms["batched"]["ms"], 3)
+    # warp execution efficiency of each form's search loop, from the instrumented kernels
+    # (one extra count each, untimed): lane-steps that placed a queen / lane-step slots
+    if not args.skip_lane_stats:
+        for fname in ([args.form] if args.skip_other_form else ["batched", "plain"]):
+            f = {"plain": nqb.FORM_PLAIN, "batched": nqb.FORM_BATCHED}[fname]
+            c, st = nqb.count_ex(n, d, device=dev, form=f, block_size=blocks[f], count_lane_steps=True)
+            assert c == count and st["nodes"] == nodes
+            forms.setdefault(fname, {})
+            forms[fname]["lane_efficiency"] = round(st["lane_efficiency"], 4)
+            forms[fname]["placed_lane_steps"] = st["placed_lane_steps"]
+            forms[fname]["lane_step_slots"] = st["lane_step_slots"]
+            forms[fname]["instrumented_kernel_ms"] = round(st["kernel_ms"], 3)
 
     # e2e: the public C ABI call with host buffers, every step
     e2e = None
@@ -356,12 +372,18 @@ def run_nqb(args):
         dist.destroy_process_group()
 
 
+def _spearman(a, b):
+    rank = lambda v: np.argsort(np.argsort(v, kind="stable"), kind="stable").astype(np.float64)
+    return float(np.corrcoef(rank(a), rank(b))[0, 1])
+
+
 def run_extras(nqb, dev, args):
     """The learned model and the other workloads of the project, beside the headline (not timed
     as the bench value): the cost model trained on 1M seeded N=18 prefixes (depth 4..8) with
-    node counts recorded by the solver; the 65,536 uneven partial boards solved through an
-    autotuned learned plan (CUDA graph) against the batched form without a model; the N=19
-    full count with learned scheduling against the plain and FIFO forms."""
+    node counts recorded by the solver, its accuracy on the N=19 depth-5 pool it never saw, and
+    an ablation of the split-and-order schedule it drives against the same pipeline driven by an
+    untrained network and by two model-free costs, on the N=19 depth-4 and N=17 depth-3 counts
+    and on the 65,536 uneven partial boards (autotuned CUDA-graph plans)."""
     out = {}
     t0 = time.perf_counter()
     boards = nqb.sample_boards(nqb.MODEL_SEED, args.model_samples, 18, 18, 4, 8)
@@ -373,28 +395,61 @@ def run_extras(nqb, dev, args):
     losses = model.train(boards[:ntr], t[:ntr], epochs=8, batch=4096, lr=2e-3)
     t2 = time.perf_counter()
     pred = model.predict(boards[ntr:])
-    out["model"] = {"samples": len(boards), "train": ntr, "label_nodes": int(nodes.sum()),
-                    "label_s": round(t1 - t0, 2), "train_s": round(t2 - t1, 2),
+    out["model"] = {"samples": len(boards), "train": ntr, "train_set": "n=18, depth 4..8 (seeded sampler)",
+                    "label_nodes": int(nodes.sum()), "label_s": round(t1 - t0, 2), "train_s": round(t2 - t1, 2),
                     "epoch_loss": [round(float(x), 4) for x in losses],
                     "val_rmse_log2": round(float(np.sqrt(np.mean((pred - t[ntr:]) ** 2))), 4),
-                    "val_std_log2": round(float(np.std(t[ntr:])), 4)}
+                    "val_std_log2": round(float(np.std(t[ntr:])), 4),
+                    "val_spearman": round(_spearman(pred, t[ntr:]), 4)}
+    # transfer to a board size the network never saw: the N=19 depth-5 pool
+    pool = nqb.generate_pool(19, 5)
+    pn, _ = nqb.record_nodes(pool, device=dev)
+    pt = np.log2(1.0 + pn.astype(np.float64))
+    pp = model.predict(pool).astype(np.float64)
+    out["model"]["n19_d5_pool"] = {"items": len(pool), "rmse_log2": round(float(np.sqrt(np.mean((pp - pt) ** 2))), 4),
+                                   "std_log2": round(float(np.std(pt)), 4), "spearman": round(_spearman(pp, pt), 4)}
+    untrained = nqb.Model(device=dev, seed=1)
+    arms = {"fifo": {}, "untrained_net": {"model": untrained}, "free_x_rows": {"sched_cost": 1},
+            "lookahead_cells": {"sched_cost": 2}, "trained_net": {"model": model}}
 
-    # uneven partial boards (65,536, n 16..20, depth 3..7)
+    # the ablation on coarse full counts: kernel + scheduling time of each arm (second of two runs)
+    abl = {}
+    for n, d in ((19, 4), (17, 3)):
+        row = {}
+        for name, kw in arms.items():
+            for _ in range(2):
+                c, st = nqb.count_ex(n, d, device=dev, form=nqb.FORM_BATCHED, **kw)
+            assert c == KAT[n]
+            row[name] = {"kernel_ms": round(st["kernel_ms"], 3), "sched_ms": round(st["sched_ms"], 3),
+                         "items": st["items"]}
+        abl[f"n{n}_d{d}"] = row
+
+    # uneven partial boards (65,536, n 16..20, depth 3..7): an autotuned plan per arm
     cb = nqb.sample_boards(nqb.BATCH_SEED, 65536, 16, 20, 3, 7)
     fifo, st_f = nqb.solve_batch(cb, device=dev, form=nqb.FORM_BATCHED)
-    tc = time.perf_counter()
-    plan = nqb.BatchPlan(cb, device=dev, model=model, autotune=True)
-    tc = time.perf_counter() - tc
-    runs = []
-    for _ in range(3):
-        got, st_p = plan.run()
-        assert np.array_equal(got, fifo)
-        runs.append(st_p["kernel_ms"])
-    out["uneven_boards"] = {"boards": len(cb), "nodes": st_f["nodes"], "sum_counts": int(fifo.sum()),
-                            "batched_fifo_ms": round(st_f["kernel_ms"], 2), "learned_plan_ms": [round(x, 2) for x in runs],
-                            "plan": plan.config(), "plan_create_s": round(tc, 2),
-                            "learned_over_fifo": round(st_f["kernel_ms"] / min(runs), 3), "bit_exact": True}
-    plan.close()
+    plain_ub, st_p0 = nqb.solve_batch(cb, device=dev, form=nqb.FORM_PLAIN)
+    assert np.array_equal(plain_ub, fifo)
+    row = {}
+    for name, kw in arms.items():
+        tc = time.perf_counter()
+        plan = nqb.BatchPlan(cb, device=dev, autotune=True, **kw)
+        tc = time.perf_counter() - tc
+        runs = []
+        for _ in range(3):
+            got, st_p = plan.run()
+            assert np.array_equal(got, fifo)
+            runs.append(st_p["kernel_ms"])
+        row[name] = {"plan_create_s": round(tc, 3), "run_ms": [round(x, 2) for x in runs], "plan": plan.config()}
+        plan.close()
+    abl["uneven_boards"] = row
+    out["ablation"] = abl
+    best = min(row["trained_net"]["run_ms"])
+    out["uneven_boards"] = {
+        "boards": len(cb), "nodes": st_f["nodes"], "sum_counts": int(fifo.sum()), "bit_exact": True,
+        "plain_ms": round(st_p0["kernel_ms"], 2), "batched_fifo_ms": round(st_f["kernel_ms"], 2),
+        "learned_plan_ms": best, "learned_over_fifo": round(st_f["kernel_ms"] / best, 3),
+        "plan_create_s": row["trained_net"]["plan_create_s"],
+        "e2e_over_fifo": round(st_f["kernel_ms"] / (1e3 * row["trained_net"]["plan_create_s"] + best), 3)}
 
     # N=19 full counts: plain, batched FIFO, batched + learned
     n19 = {}
@@ -406,15 +461,8 @@ def run_extras(nqb, dev, args):
         n19[f"d{d}"] = {"plain_ms": round(s0["kernel_ms"], 2), "batched_ms": round(s1["kernel_ms"], 2),
                         "learned_ms": round(s2["kernel_ms"], 2), "learned_sched_ms": round(s2["sched_ms"], 2),
                         "learned_items": s2["items"], "learned_over_plain": round(s0["kernel_ms"] / s2["kernel_ms"], 3)}
-    pool = nqb.generate_pool(19, 5)
-    pn, _ = nqb.record_nodes(pool, device=dev)
-    pt = np.log2(1.0 + pn.astype(np.float64))
-    pp = model.predict(pool).astype(np.float64)
-    n19["rmse_log2_on_d5_pool"] = round(float(np.sqrt(np.mean((pp - pt) ** 2))), 4)
-    rank = lambda v: np.argsort(np.argsort(v)).astype(np.float64)  # ties are negligible here
-    n19["spearman_on_d5_pool"] = round(float(np.corrcoef(rank(pp), rank(pt))[0, 1]), 4)
-    n19["std_log2_on_d5_pool"] = round(float(np.std(pt)), 4)
     out["n19"] = n19
+    untrained.close()
     model.close()
     return out
 
@@ -485,9 +533,10 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-step-seconds", type=float, default=8.0)
     ap.add_argument("--ref-cuda", type=int, default=1)
-    ap.add_argument("--ref-cuda-n", type=int, default=19)
+    ap.add_argument("--ref-cuda-n", type=int, default=21)
     ap.add_argument("--ref-cuda-d", type=int, default=7)
     ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-lane-stats", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch autotuner (default block sizes)")
     args = ap.parse_args()

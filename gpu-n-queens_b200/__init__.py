@@ -42,7 +42,8 @@ class Opts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("form", ctypes.c_int), ("block_size", ctypes.c_int),
                 ("count_unit_nodes", ctypes.c_int), ("max_split_rounds", ctypes.c_int),
                 ("split_factor", ctypes.c_int), ("model", ctypes.c_void_p), ("host_pool", ctypes.c_int),
-                ("autotune", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
+                ("autotune", ctypes.c_int), ("count_lane_steps", ctypes.c_int), ("sched_cost", ctypes.c_int),
+                ("reserved", ctypes.c_int * 4)]
 
 
 class Stats(ctypes.Structure):
@@ -50,12 +51,14 @@ class Stats(ctypes.Structure):
                 ("gen_ms", ctypes.c_double), ("h2d_ms", ctypes.c_double), ("kernel_ms", ctypes.c_double),
                 ("wall_ms", ctypes.c_double), ("pregen_depth", ctypes.c_uint32),
                 ("kernel_launches", ctypes.c_uint32), ("items", ctypes.c_uint64), ("sched_ms", ctypes.c_double),
-                ("block_size", ctypes.c_uint32), ("form", ctypes.c_int32)]
+                ("block_size", ctypes.c_uint32), ("form", ctypes.c_int32), ("placed_lane_steps", ctypes.c_uint64),
+                ("lane_step_slots", ctypes.c_uint64)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
         if d["unit_nodes"] == 2 ** 64 - 1:
             d["unit_nodes"] = None
+        d["lane_efficiency"] = (self.placed_lane_steps / self.lane_step_slots) if self.lane_step_slots else None
         return d
 
 
@@ -102,6 +105,8 @@ def lib():
                                                 ctypes.c_uint, vp]),
             "nqb_batched_launch": (ctypes.c_int, [vp, ctypes.c_uint64, vp, vp, vp, ctypes.c_int, ctypes.c_uint,
                                                   vp]),
+            "nqb_batched_launch_ex": (ctypes.c_int, [vp, ctypes.c_uint64, vp, vp, ctypes.c_uint64, vp, vp,
+                                                     ctypes.c_int, ctypes.c_uint, ctypes.c_uint, vp]),
             "nqb_generate_pool_placements": (ctypes.c_int, [ctypes.c_uint, ctypes.c_uint, ctypes.POINTER(vp), u64p]),
             "nqb_states_from_placements": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.c_int, vp]),
             "nqb_write_state_file": (ctypes.c_int, [ctypes.c_char_p, vp, ctypes.c_uint64, ctypes.c_uint,
@@ -139,7 +144,7 @@ def _check(status, what):
 
 
 def make_opts(device=0, form=FORM_PLAIN, block_size=0, count_unit_nodes=False, model=None, max_split_rounds=-1,
-              split_factor=0, host_pool=False, autotune=False):
+              split_factor=0, host_pool=False, autotune=False, count_lane_steps=False, sched_cost=0):
     o = Opts()
     lib().nqb_default_opts(ctypes.byref(o))
     o.device, o.form, o.block_size = device, form, block_size
@@ -147,6 +152,8 @@ def make_opts(device=0, form=FORM_PLAIN, block_size=0, count_unit_nodes=False, m
     o.model = model.handle if model is not None else None
     o.host_pool = int(host_pool)
     o.autotune = int(autotune)
+    o.count_lane_steps = int(count_lane_steps)
+    o.sched_cost = int(sched_cost)
     return o
 
 
@@ -411,6 +418,18 @@ def batched_launch(d_items_ptr, count, d_head_ptr, d_out_ptr, d_order_ptr=None, 
                                     stack_depth, stream or None), "nqb_batched_launch")
 
 
+BATCHED_SCRATCH_BYTES = 64 + 32 * 65536  # NQB_BATCHED_SCRATCH_BYTES
+
+
+def batched_launch_ex(d_items_ptr, count, d_scratch_ptr, scratch_bytes, d_out_ptr, d_order_ptr=None,
+                      d_lane_stats_ptr=None, block_size=0, stack_depth=0, wait_limit=0, stream=0):
+    """Launches the batched kernel with work stealing across warps (see nqb_batched_launch_ex);
+    the caller reads the launch's error flags from d_out[3]."""
+    _check(lib().nqb_batched_launch_ex(d_items_ptr, count, d_order_ptr, d_scratch_ptr, scratch_bytes, d_out_ptr,
+                                       d_lane_stats_ptr, block_size, stack_depth, wait_limit, stream or None),
+           "nqb_batched_launch_ex")
+
+
 MODEL_INPUTS, MODEL_PARAMS = 112, 31105
 
 
@@ -510,7 +529,7 @@ class BatchPlan:
     """A board set solved repeatedly through one captured CUDA graph (nqb_batch_plan_*)."""
 
     def __init__(self, boards, device=0, model=None, autotune=True, block_size=0, split_factor=0,
-                 max_split_rounds=-1):
+                 max_split_rounds=-1, sched_cost=0):
         L = lib()
         vp = ctypes.c_void_p
         for name, (res, args) in {
@@ -526,7 +545,7 @@ class BatchPlan:
         self.handle = None
         self.boards = np.ascontiguousarray(boards, dtype=STATE_DTYPE)
         o = make_opts(device=device, form=FORM_BATCHED, block_size=block_size, model=model,
-                      max_split_rounds=max_split_rounds, split_factor=split_factor)
+                      max_split_rounds=max_split_rounds, split_factor=split_factor, sched_cost=sched_cost)
         h = ctypes.c_void_p()
         _check(L.nqb_batch_plan_create(self.boards.ctypes.data, len(self.boards), ctypes.byref(o), int(autotune),
                                        ctypes.byref(h)), "nqb_batch_plan_create")

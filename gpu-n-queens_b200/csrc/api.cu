@@ -94,9 +94,11 @@ int solve_device_states(Scope& sc, const nqb_state* d_states, uint64_t count, un
     const bool batched = o.form == NQB_FORM_BATCHED;
     if (o.form != NQB_FORM_PLAIN && !batched) return NQB_E_INVALID;
     if (batched && count > (1ull << 31)) return NQB_E_RANGE;
-    unsigned long long* d_out = nullptr;  // 4 result words, then the queue head
+    // 4 result words, 2 lane-step counters, 2 spare, then the batched launch's scratch
+    unsigned long long* d_out = nullptr;
     unsigned long long* d_per = nullptr;
-    NQB_TRY(sc.alloc(&d_out, 5 * sizeof(unsigned long long)));
+    const size_t out_bytes = 8 * sizeof(unsigned long long) + (batched ? kBatchedScratchBytes : 0);
+    NQB_TRY(sc.alloc(&d_out, out_bytes));
     if (per_state) NQB_TRY(sc.alloc(&d_per, count * sizeof(unsigned long long)));
     unsigned long long* d_per_nodes = nullptr;
     if (per_state_nodes) {
@@ -104,11 +106,11 @@ int solve_device_states(Scope& sc, const nqb_state* d_states, uint64_t count, un
         NQB_TRY(sc.alloc(&d_per_nodes, count * sizeof(unsigned long long)));
         NQB_TRY(cuda_status(cudaMemsetAsync(d_per_nodes, 0, count * sizeof(unsigned long long), sc.stream)));
     }
-    uint32_t* d_head = reinterpret_cast<uint32_t*>(d_out + 4);
+    unsigned long long* d_lanes = o.count_lane_steps ? d_out + 4 : nullptr;
     cudaEvent_t e1, e2;
     NQB_TRY(sc.event(&e1));
     NQB_TRY(sc.event(&e2));
-    NQB_TRY(cuda_status(cudaMemsetAsync(d_out, 0, 5 * sizeof(unsigned long long), sc.stream)));
+    NQB_TRY(cuda_status(cudaMemsetAsync(d_out, 0, out_bytes, sc.stream)));
     if (d_per) NQB_TRY(cuda_status(cudaMemsetAsync(d_per, 0, count * sizeof(unsigned long long), sc.stream)));
     NQB_TRY(cuda_status(cudaEventRecord(e1, sc.stream)));
     unsigned launches = 0;
@@ -116,16 +118,20 @@ int solve_device_states(Scope& sc, const nqb_state* d_states, uint64_t count, un
     sched.items = count;
     if (count) {
         if (batched) {
-            NQB_TRY(launch_batched_scheduled(d_states, (uint32_t)count, nullptr, d_head, d_out, d_per, d_per_nodes, o,
-                                             depth, sc.device, sc.stream, &launches, &sched));
+            NQB_TRY(launch_batched_scheduled(d_states, (uint32_t)count, nullptr, d_out + 8, kBatchedScratchBytes, d_out,
+                                             d_per, d_per_nodes, o, depth, sc.device, sc.stream, &launches, &sched,
+                                             d_lanes));
         } else {
             NQB_TRY(launch_plain(d_states, count, d_out, d_per, o.block_size, o.count_unit_nodes != 0, depth,
-                                 sc.stream, &launches));
+                                 sc.stream, &launches, d_lanes));
         }
     }
     NQB_TRY(cuda_status(cudaEventRecord(e2, sc.stream)));
+    unsigned long long lanes[2] = {0, 0};
     NQB_TRY(cuda_status(cudaMemcpyAsync(totals, d_out, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                                         sc.stream)));
+    if (d_lanes)
+        NQB_TRY(cuda_status(cudaMemcpyAsync(lanes, d_lanes, sizeof(lanes), cudaMemcpyDeviceToHost, sc.stream)));
     if (per_state)
         NQB_TRY(cuda_status(cudaMemcpyAsync(per_state, d_per, count * sizeof(unsigned long long),
                                             cudaMemcpyDeviceToHost, sc.stream)));
@@ -133,6 +139,7 @@ int solve_device_states(Scope& sc, const nqb_state* d_states, uint64_t count, un
         NQB_TRY(cuda_status(cudaMemcpyAsync(per_state_nodes, d_per_nodes, count * sizeof(unsigned long long),
                                             cudaMemcpyDeviceToHost, sc.stream)));
     NQB_TRY(cuda_status(cudaStreamSynchronize(sc.stream)));
+    if (totals[3] & 4) return NQB_E_STALL;
     if (totals[3]) return NQB_E_DEVICE;
     if (st) {
         float h2d = 0, ker = 0;
@@ -148,6 +155,8 @@ int solve_device_states(Scope& sc, const nqb_state* d_states, uint64_t count, un
         st->sched_ms = sched.sched_ms;
         st->block_size = (uint32_t)(o.block_size ? o.block_size : 128);
         st->form = o.form;
+        st->placed_lane_steps = lanes[0];
+        st->lane_step_slots = lanes[1];
     }
     return NQB_OK;
 }
@@ -469,9 +478,21 @@ int nqb_batched_launch(const nqb_state* d_items, uint64_t count, const uint32_t*
     if (count > (1ull << 31)) return NQB_E_RANGE;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return NQB_E_NODEVICE;
-    return launch_batched(d_items, (uint32_t)count, d_order, nullptr, d_head,
+    return launch_batched(d_items, (uint32_t)count, d_order, nullptr, d_head, sizeof(uint32_t),
                           reinterpret_cast<unsigned long long*>(d_out), nullptr, nullptr, block_size, stack_depth, dev,
                           static_cast<cudaStream_t>(stream), nullptr);
+}
+
+int nqb_batched_launch_ex(const nqb_state* d_items, uint64_t count, const uint32_t* d_order, void* d_scratch,
+                          uint64_t scratch_bytes, uint64_t* d_out, uint64_t* d_lane_stats, int block_size,
+                          unsigned stack_depth, unsigned wait_limit, void* stream) {
+    if (count > (1ull << 31)) return NQB_E_RANGE;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return NQB_E_NODEVICE;
+    return launch_batched(d_items, (uint32_t)count, d_order, nullptr, d_scratch, (size_t)scratch_bytes,
+                          reinterpret_cast<unsigned long long*>(d_out), nullptr, nullptr, block_size, stack_depth, dev,
+                          static_cast<cudaStream_t>(stream), nullptr,
+                          reinterpret_cast<unsigned long long*>(d_lane_stats), wait_limit);
 }
 
 int nqb_generate_pool_device(unsigned n, unsigned depth, nqb_state** d_states, uint64_t* count, void* stream) {

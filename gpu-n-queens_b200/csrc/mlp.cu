@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(128) gemm_tc(const __half* __restrict__ A, lon
     uint32_t tmem = 0;
     asm volatile("ld.shared.u32 %0, [%1];" : "=r"(tmem) : "r"(tmem_slot) : "memory");
     uint32_t phase = 0;
-    bool failed = false;
+    bool failed = false, undrained = false;
     const int i = m0 + (int)t;  // this thread's row of A and of C
     const int j = (int)t;       // this thread's row of B (column of C)
     for (int k0 = kb; k0 < ke && !failed; k0 += kGemmK) {
@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(128) gemm_tc(const __half* __restrict__ A, lon
         }
         const bool ok = mbar_wait(bar, phase);
         if (__syncthreads_or(!ok)) {  // timed out: drain the MMAs in flight (bounded), then leave
-            mbar_wait(bar, phase);
+            undrained = !__syncthreads_and(mbar_wait(bar, phase));
             failed = true;
             break;
         }
@@ -238,7 +238,9 @@ __global__ void __launch_bounds__(128) gemm_tc(const __half* __restrict__ A, lon
             __syncthreads();
         }
     }
-    if (failed && t == 0) atomicOr(err, 1u);
+    // bit 0: a completion wait timed out; bit 1: the drain timed out too, so products may still
+    // have been in flight when the tensor memory was freed
+    if (failed && t == 0) atomicOr(err, undrained ? 3u : 1u);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -460,7 +462,7 @@ __global__ void __launch_bounds__(128) predict_kernel(const uint4* __restrict__ 
     asm volatile("ld.shared.u32 %0, [%1];" : "=r"(tmem) : "r"(tmem_slot) : "memory");
     const uint32_t my_lanes = tmem + ((warp * 32u) << 16);
     uint32_t phase = 0;
-    bool failed = false;
+    bool failed = false, undrained = false;
 
     for (uint32_t tile = blockIdx.x; (uint64_t)tile * kTileRows < count && !failed; tile += gridDim.x) {
         const uint64_t i = (uint64_t)tile * kTileRows + t;
@@ -491,7 +493,7 @@ __global__ void __launch_bounds__(128) predict_kernel(const uint4* __restrict__ 
             }
             const bool ok = wait_limit ? mbar_wait(bar, phase, wait_limit, true) : mbar_wait(bar, phase);
             if (__syncthreads_or(!ok)) {  // timed out: drain the MMAs in flight (bounded), then leave
-                mbar_wait(bar, phase);
+                undrained = !__syncthreads_and(mbar_wait(bar, phase));
                 failed = true;
                 break;
             }
@@ -523,7 +525,9 @@ __global__ void __launch_bounds__(128) predict_kernel(const uint4* __restrict__ 
         if (!failed && i < count) out[i] = sum + vec[3 * kH];
         __syncthreads();  // the operand tile and the accumulator are free for the next tile
     }
-    if (failed && t == 0) atomicOr(err, 1u);
+    // bit 0: a completion wait timed out; bit 1: the drain timed out too, so products may still
+    // have been in flight when the tensor memory was freed
+    if (failed && t == 0) atomicOr(err, undrained ? 3u : 1u);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -576,7 +580,7 @@ struct Work {
         unsigned h = 0;
         int st = cuda_status(cudaMemcpyAsync(&h, err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
         if (!st) st = cuda_status(cudaStreamSynchronize(s));
-        return st ? st : (h ? NQB_E_STALL : NQB_OK);
+        return st ? st : (h & 2u) ? NQB_E_DEVICE : (h ? NQB_E_STALL : NQB_OK);
     }
     ~Work() {
         for (void* p : owned) cudaFree(p);
@@ -916,7 +920,7 @@ int model_predict_device(const nqb_model* m, const nqb_state* d_states, uint32_t
     if (!st) st = cuda_status(cudaMemcpyAsync(&h_err, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     if (!st) st = cuda_status(cudaStreamSynchronize(s));
     dev_free(d_err, s);
-    if (!st && h_err) st = NQB_E_STALL;
+    if (!st && h_err) st = (h_err & 2u) ? NQB_E_DEVICE : NQB_E_STALL;
     return st;
 }
 

@@ -10,7 +10,7 @@ namespace nqb {
 namespace mlp {
 
 // Network 112 -> 128 -> 128 -> 1, GELU after both hidden layers.
-constexpr int kIn = 112;  // 3 x 32 mask bits + 4 scalars, zero-padded to a multiple of 16
+constexpr int kIn = 112;  // 96 + 6 board-relative features (see feature()), zero-padded to a multiple of 16
 constexpr int kH = 128;
 constexpr int kW1Size = kIn * kH;
 constexpr int kW1 = 0;  // offsets of the parameters in the flat fp32 vector
@@ -33,28 +33,50 @@ __device__ __forceinline__ float gelu_grad(float x) {
     return 0.5f * (1.0f + th) + 0.5f * x * (1.0f - th * th) * kGeluC * (1.0f + 3.0f * kGeluA * x * x);
 }
 
-// Feature j of a state {cols, ldiag, rdiag, meta}: bits 0..31 of the free-column mask,
-// bits 0..31 of the ldiag mask restricted to the board, bits 0..31 of rdiag, then n/32,
-// row/32, free columns/32 and candidates of the next row/32; zero beyond.
+__host__ __device__ __forceinline__ uint32_t popc32(uint32_t v) {
+#ifdef __CUDA_ARCH__
+    return __popc(v);
+#else
+    return (uint32_t)__builtin_popcount(v);
+#endif
+}
+
+// Cells of row `row + k` that the queens above leave free (k = 0: the next row's candidates).
+__host__ __device__ __forceinline__ uint32_t free_cells_below(uint32_t nc, uint32_t ld, uint32_t rd, uint32_t k) {
+    return popc32(nc & ~((ld << k) | (rd >> k)));
+}
+
+// Feature j of a state {cols, ldiag, rdiag, meta}.  Every feature is relative to the board, so
+// one network ranks states of different board sizes:
+//   0..31   free cells of each of the next 32 rows under the queens already placed
+//           (row + k for feature k; 0 beyond the last row), / 32
+//   32..63  the free-column mask, centred on the board (bit i at 16 - n/2 + i)
+//   64..95  the next row's candidate mask, centred the same way
+//   96      rows left / 32        97  free columns / 32      98  next-row candidates / 32
+//   99      n / 32                100 row / 32               101 sum of features 0..31 x 32 / 256
+// then zero.  All are small integers over powers of two, exact in fp16.
 __host__ __device__ __forceinline__ float feature(const uint4 st, int j) {
     const uint32_t n = (st.w >> 8) & 0xFFu;
     const uint32_t row = st.w & 0xFFu;
     const uint32_t mask = n >= 32 ? 0xFFFFFFFFu : ((1u << n) - 1u);
     const uint32_t nc = mask & ~st.x;
-    if (j < 32) return (float)((nc >> j) & 1u);
-    if (j < 64) return (float)(((st.y & mask) >> (j - 32)) & 1u);
-    if (j < 96) return (float)(((st.z & mask) >> (j - 64)) & 1u);
+    const uint32_t left = n > row ? n - row : 0u;
+    const uint32_t shift = 16u - (n >> 1);
+    if (j < 32) return (uint32_t)j < left ? free_cells_below(nc, st.y, st.z, (uint32_t)j) / 32.0f : 0.0f;
+    if (j < 64) return (float)(((nc << shift) >> (j - 32)) & 1u);
     const uint32_t avail = nc & ~(st.y | st.z);
+    if (j < 96) return (float)(((avail << shift) >> (j - 64)) & 1u);
     switch (j) {
-        case 96: return n / 32.0f;
-        case 97: return row / 32.0f;
-#ifdef __CUDA_ARCH__
-        case 98: return __popc(nc) / 32.0f;
-        case 99: return __popc(avail) / 32.0f;
-#else
-        case 98: return __builtin_popcount(nc) / 32.0f;
-        case 99: return __builtin_popcount(avail) / 32.0f;
-#endif
+        case 96: return left / 32.0f;
+        case 97: return popc32(nc) / 32.0f;
+        case 98: return popc32(avail) / 32.0f;
+        case 99: return n / 32.0f;
+        case 100: return row / 32.0f;
+        case 101: {
+            uint32_t sum = 0;
+            for (uint32_t k = 0; k < left && k < 32; ++k) sum += free_cells_below(nc, st.y, st.z, k);
+            return sum / 256.0f;
+        }
         default: return 0.0f;
     }
 }

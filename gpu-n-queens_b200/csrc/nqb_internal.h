@@ -42,18 +42,33 @@ unsigned host_threads();
 unsigned max_stack_depth(const nqb_state* states, uint64_t count);
 
 // Plain search kernel (plain.cu).  d_out: {weighted count, nodes, unit nodes, error flags}.
-// d_per_state (optional): weight x completions per state.
+// d_per_state (optional): weight x completions per state.  d_lane_stats (optional): the
+// instrumented kernel adds {lane-steps that placed a queen, lane-step slots} into it.
 int launch_plain(const nqb_state* d_states, uint64_t count, unsigned long long* d_out,
                  unsigned long long* d_per_state, int block_size, bool count_unit, unsigned stack_depth,
-                 cudaStream_t stream, unsigned* launches);
+                 cudaStream_t stream, unsigned* launches, unsigned long long* d_lane_stats = nullptr);
 
-// Batched (persistent, work-queue) search kernel (batched.cu).  d_head: queue head,
-// zeroed before launch.  d_order (optional): queue position -> item; d_board_of
-// (optional): item -> output slot.  d_out: {weighted count, nodes, 0, error flags}.
+// Scratch of one batched launch (zeroed before it): 64 bytes of control words (word 0 is
+// the item queue head), then the steal ring, 32 bytes a slot.  Scratch of 4 bytes (the
+// head alone) launches without stealing across warps.
+constexpr size_t kBatchedCtlBytes = 64;
+constexpr size_t kBatchedSlotBytes = 32;
+constexpr uint32_t kBatchedRingSlots = 1u << 16;  // the library's own launches: 2 MB
+constexpr size_t kBatchedScratchBytes = kBatchedCtlBytes + kBatchedRingSlots * kBatchedSlotBytes;
+constexpr uint32_t kBatchedWaitLimit = 1u << 18;  // polls without progress (about 2 s of backoff)
+// Ring slots a scratch buffer of `scratch_bytes` holds (a power of two; 0 = no ring).
+uint32_t batched_ring_slots(size_t scratch_bytes);
+
+// Batched (persistent, work-queue) search kernel (batched.cu).  d_scratch as above.
+// d_order (optional): queue position -> item; d_board_of (optional): item -> output slot.
+// d_out: {weighted count, nodes, 0, error flags}.  d_lane_stats as for launch_plain.
+// wait_limit: polls without progress before a wait of the work stealing gives up (0 =
+// kBatchedWaitLimit).
 int launch_batched(const nqb_state* d_items, uint32_t n_items, const uint32_t* d_order, const uint32_t* d_board_of,
-                   uint32_t* d_head, unsigned long long* d_out, unsigned long long* d_per_board,
-                   unsigned long long* d_per_board_nodes, int block_size, unsigned stack_depth, int device,
-                   cudaStream_t stream, unsigned* launches);
+                   void* d_scratch, size_t scratch_bytes, unsigned long long* d_out,
+                   unsigned long long* d_per_board, unsigned long long* d_per_board_nodes, int block_size,
+                   unsigned stack_depth, int device, cudaStream_t stream, unsigned* launches,
+                   unsigned long long* d_lane_stats = nullptr, uint32_t wait_limit = 0);
 
 // Items after learned scheduling: the caller's arrays, or split / ordered device copies
 // owned by the schedule until release() (stream-ordered frees).
@@ -82,10 +97,11 @@ struct SchedInfo {
     uint64_t items = 0;     // items given to the search kernel
     double sched_ms = 0.0;  // prediction + splitting + ordering (device time)
 };
-int launch_batched_scheduled(const nqb_state* d_items, uint32_t n, const uint32_t* d_board, uint32_t* d_head,
-                             unsigned long long* d_out, unsigned long long* d_per_board,
+int launch_batched_scheduled(const nqb_state* d_items, uint32_t n, const uint32_t* d_board, void* d_scratch,
+                             size_t scratch_bytes, unsigned long long* d_out, unsigned long long* d_per_board,
                              unsigned long long* d_per_board_nodes, const nqb_opts& o, unsigned stack_depth,
-                             int device, cudaStream_t s, unsigned* launches, SchedInfo* info);
+                             int device, cudaStream_t s, unsigned* launches, SchedInfo* info,
+                             unsigned long long* d_lane_stats = nullptr);
 
 // Stream-ordered device allocation from the library's pool on the current device
 // (devmem.cu); release with dev_free on a stream.  Freed memory stays cached for later
@@ -101,6 +117,9 @@ int dev_alloc(T** p, size_t bytes, cudaStream_t s) {
 void dev_free(void* p, cudaStream_t s);
 
 int cuda_status(cudaError_t e);
+
+// Unique id of the calling thread's current CUDA context, 0 when none (devmem.cu).
+unsigned long long current_context_id();
 
 // Learned cost model (mlp.cu): predicted log2(1 + nodes) of `count` device states.
 int model_predict_device(const nqb_model* m, const nqb_state* d_states, uint32_t count, float* d_out, cudaStream_t s,

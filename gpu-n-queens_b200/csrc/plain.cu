@@ -18,7 +18,7 @@ namespace {
 
 constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr int kUnroll = 16;
-constexpr uint32_t kEpoch = 1u << 27;  // votes between folds: kUnroll x kEpoch < 2^32
+constexpr uint32_t kEpoch = 1u << 22;  // votes between folds: 31 nodes x kUnroll x kEpoch < 2^32
 
 // Error flags written to out[3].
 constexpr unsigned kErrStack = 1u;  // a state needed a deeper stack than provided
@@ -26,11 +26,15 @@ constexpr unsigned kErrBound = 2u;  // checked builds: a push would have passed 
 
 // per_state (optional): weight x completions of each state, for per-board results.
 // UNIT: also count placements made by unit-row propagation (the reference's split of
-// nodes; a row entered with exactly one free column, other than the start row).
-template <int BLOCK, bool UNIT>
+// nodes: the candidate of a row entered with exactly one candidate, other than the start
+// row).  lane_stats (optional, LANES builds): {lane-steps that placed a queen, lane-step
+// slots issued (32 per warp step)}: their ratio is the search loop's warp execution
+// efficiency in active lanes.
+template <int BLOCK, bool UNIT, bool LANES>
 __global__ void __launch_bounds__(BLOCK) plain_search_kernel(const uint4* __restrict__ states, uint32_t count,
                                                              unsigned long long* __restrict__ out,
                                                              unsigned long long* __restrict__ per_state,
+                                                             unsigned long long* __restrict__ lane_stats,
                                                              uint32_t stack_depth) {
     extern __shared__ uint4 stack[];  // [stack_depth + 1][BLOCK]; row 0 holds the sentinels
     constexpr int kStride = BLOCK * 16;
@@ -54,34 +58,45 @@ __global__ void __launch_bounds__(BLOCK) plain_search_kernel(const uint4* __rest
             bad = true;
             lane_park(s, base);
             s.sols = 0;
+            s.nodes = 0;
         }
     }
-    unsigned long long sols = 0, nodes = 0;
-    uint32_t unit = 0;
-    bool first = true;
+    unsigned long long sols = 0, nodes = 0, unit64 = 0, placed64 = 0, votes = 0;
+    uint32_t unit = 0, placed = 0;
     uint32_t epoch = kEpoch;
     while (!__all_sync(kFull, s.avail == 0 && s.sp == base)) {
         if (--epoch == 0) {  // fold lane counters before they can wrap
             sols += s.sols;
             nodes += s.nodes;
             s.sols = s.nodes = 0;
+            unit64 += unit;
+            placed64 += placed;
+            unit = placed = 0;
             epoch = kEpoch;
         }
+        if (LANES) ++votes;
 #pragma unroll
         for (int u = 0; u < kUnroll; ++u) {
-            if (UNIT) {
-                unit += (!first && s.avail != 0 && (s.avail & (s.avail - 1u)) == 0);
-                first = false;
-            }
-            search_step<kStride>(s, base, top);
+            const StepInfo si = search_step<kStride>(s, base, top);
+            if (UNIT) unit += (si.cand == 1u);
+            if (LANES) placed += (si.placed != 0u);
         }
     }
     sols += s.sols;
     nodes += s.nodes;
+    unit64 += unit;
+    placed64 += placed;
+    if (LANES) {
+        const unsigned long long pw = warp_sum_u64(placed64);
+        if ((tid & 31) == 0) {
+            atomicAdd(lane_stats + 0, pw);
+            atomicAdd(lane_stats + 1, 32ull * kUnroll * votes);
+        }
+    }
 
     unsigned long long c = sols * weight;
     if (per_state && gi < count) per_state[gi] = c;
-    unsigned long long un = unit;
+    unsigned long long un = unit64;
     c = warp_sum_u64(c);
     nodes = warp_sum_u64(nodes);
     if (UNIT) un = warp_sum_u64(un);
@@ -115,10 +130,11 @@ __global__ void __launch_bounds__(BLOCK) plain_search_kernel(const uint4* __rest
     }
 }
 
-template <int BLOCK, bool UNIT>
+template <int BLOCK, bool UNIT, bool LANES>
 int launch_t(const nqb_state* d_states, uint64_t count, unsigned long long* d_out,
-             unsigned long long* d_per_state, unsigned stack_depth, cudaStream_t stream, unsigned* launches) {
-    auto kern = plain_search_kernel<BLOCK, UNIT>;
+             unsigned long long* d_per_state, unsigned long long* d_lanes, unsigned stack_depth,
+             cudaStream_t stream, unsigned* launches) {
+    auto kern = plain_search_kernel<BLOCK, UNIT, LANES>;
     // Room for the stack (with its sentinel row), and for 4 x (BLOCK/32) reduction words.
     const size_t smem = std::max<size_t>((size_t)(stack_depth + 1) * BLOCK * sizeof(uint4),
                                          4 * (BLOCK / 32) * sizeof(unsigned long long));
@@ -131,7 +147,7 @@ int launch_t(const nqb_state* d_states, uint64_t count, unsigned long long* d_ou
         const uint32_t c = (uint32_t)std::min<uint64_t>(kChunk, count - off);
         const unsigned grid = (c + BLOCK - 1) / BLOCK;
         kern<<<grid, BLOCK, smem, stream>>>(base + off, c, d_out, d_per_state ? d_per_state + off : nullptr,
-                                            stack_depth);
+                                            d_lanes, stack_depth);
         e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_status(e);
         if (launches) (*launches)++;
@@ -139,11 +155,26 @@ int launch_t(const nqb_state* d_states, uint64_t count, unsigned long long* d_ou
     return NQB_OK;
 }
 
+template <int BLOCK>
+int launch_block(const nqb_state* d_states, uint64_t count, unsigned long long* d_out,
+                 unsigned long long* d_per_state, unsigned long long* d_lanes, bool count_unit, unsigned stack_depth,
+                 cudaStream_t stream, unsigned* launches) {
+    if (d_lanes)
+        return count_unit ? launch_t<BLOCK, true, true>(d_states, count, d_out, d_per_state, d_lanes, stack_depth,
+                                                        stream, launches)
+                          : launch_t<BLOCK, false, true>(d_states, count, d_out, d_per_state, d_lanes, stack_depth,
+                                                         stream, launches);
+    return count_unit ? launch_t<BLOCK, true, false>(d_states, count, d_out, d_per_state, nullptr, stack_depth,
+                                                     stream, launches)
+                      : launch_t<BLOCK, false, false>(d_states, count, d_out, d_per_state, nullptr, stack_depth,
+                                                      stream, launches);
+}
+
 }  // namespace
 
 int launch_plain(const nqb_state* d_states, uint64_t count, unsigned long long* d_out,
                  unsigned long long* d_per_state, int block_size, bool count_unit, unsigned stack_depth,
-                 cudaStream_t stream, unsigned* launches) {
+                 cudaStream_t stream, unsigned* launches, unsigned long long* d_lane_stats) {
     if (!d_out || (count && !d_states)) return NQB_E_INVALID;
     if (count == 0) return NQB_OK;
     if (stack_depth == 0) stack_depth = NQB_MAX_N - 1;
@@ -151,14 +182,14 @@ int launch_plain(const nqb_state* d_states, uint64_t count, unsigned long long* 
     if (block_size == 0) block_size = 128;
     switch (block_size) {
         case 64:
-            return count_unit ? launch_t<64, true>(d_states, count, d_out, d_per_state, stack_depth, stream, launches)
-                              : launch_t<64, false>(d_states, count, d_out, d_per_state, stack_depth, stream, launches);
+            return launch_block<64>(d_states, count, d_out, d_per_state, d_lane_stats, count_unit, stack_depth,
+                                    stream, launches);
         case 128:
-            return count_unit ? launch_t<128, true>(d_states, count, d_out, d_per_state, stack_depth, stream, launches)
-                              : launch_t<128, false>(d_states, count, d_out, d_per_state, stack_depth, stream, launches);
+            return launch_block<128>(d_states, count, d_out, d_per_state, d_lane_stats, count_unit, stack_depth,
+                                     stream, launches);
         case 256:
-            return count_unit ? launch_t<256, true>(d_states, count, d_out, d_per_state, stack_depth, stream, launches)
-                              : launch_t<256, false>(d_states, count, d_out, d_per_state, stack_depth, stream, launches);
+            return launch_block<256>(d_states, count, d_out, d_per_state, d_lane_stats, count_unit, stack_depth,
+                                     stream, launches);
         default:
             return NQB_E_INVALID;
     }

@@ -1,12 +1,14 @@
 // Batch plans: a batch of uneven partial boards solved repeatedly through one captured CUDA
 // graph, with the launch configuration chosen by timing (the autotuner).
 //
-// Creation uploads the boards once, builds the learned schedule (split + order, schedule.cu)
-// for each candidate split factor, and captures per candidate block size the whole solve
-// (zero the per-board counts and the queue head, one batched-kernel launch, read the
-// results back into pinned host memory) into a CUDA graph.  With autotuning every
-// (block size, split factor) candidate is replayed once and timed with CUDA events; the
-// fastest is kept.  A run is then a single cudaGraphLaunch.
+// Creation uploads the boards once.  With autotuning every (block size, split factor)
+// candidate is first timed with CUDA events on a stride sample of the boards (at most about
+// 4,096 of them, each with the sample's own learned schedule), which costs a fraction of one
+// solve of the batch.  The learned schedule (split + order, schedule.cu) of the batch is then
+// built for the winning split factor, and the whole solve (zero the per-board counts and the
+// launch scratch, one batched-kernel launch, read the results back into pinned host memory)
+// is captured into a CUDA graph.  A run is then a single cudaGraphLaunch.
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -20,7 +22,7 @@ struct nqb_batch_plan {
     unsigned stack_depth = 0;
     nqb_state* d_boards = nullptr;
     unsigned long long* d_per = nullptr;  // per-board weighted counts
-    unsigned long long* d_out = nullptr;  // {count, nodes, unit, error flags, queue head}
+    unsigned long long* d_out = nullptr;  // {count, nodes, unit, error flags}, 4 spare words, batched scratch
     unsigned long long* d_split = nullptr;
     unsigned long long* h_per = nullptr;  // pinned
     unsigned long long* h_out = nullptr;  // pinned
@@ -36,15 +38,17 @@ namespace {
 
 using nqb::cuda_status;
 
-// Zero the outputs and the queue head, launch, read back: the sequence a run replays.
+// Zero the outputs and the launch scratch, launch, read back: the sequence a run replays.
 int solve_sequence(nqb_batch_plan* p, int block) {
     cudaStream_t s = p->s;
-    uint32_t* head = reinterpret_cast<uint32_t*>(p->d_out + 4);
     int st = cuda_status(cudaMemsetAsync(p->d_per, 0, p->count * sizeof(unsigned long long), s));
-    if (!st) st = cuda_status(cudaMemsetAsync(p->d_out, 0, 5 * sizeof(unsigned long long), s));
+    if (!st)
+        st = cuda_status(
+            cudaMemsetAsync(p->d_out, 0, 8 * sizeof(unsigned long long) + nqb::kBatchedScratchBytes, s));
     if (!st)
         st = nqb::launch_batched(reinterpret_cast<const nqb_state*>(p->sch.items), p->sch.n, p->sch.order,
-                                 p->sch.board, head, p->d_out, p->d_per, nullptr, block, p->stack_depth, p->device, s,
+                                 p->sch.board, p->d_out + 8, nqb::kBatchedScratchBytes, p->d_out, p->d_per, nullptr,
+                                 block, p->stack_depth, p->device, s,
                                  nullptr);
     if (!st)
         st = cuda_status(
@@ -101,6 +105,67 @@ int build_schedule(nqb_batch_plan* p, const nqb_opts& o, int factor) {
     return st;
 }
 
+__global__ void stride_gather(const uint4* __restrict__ in, uint64_t count, uint64_t stride, uint4* __restrict__ out) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) out[i] = in[i * stride];
+}
+
+// Boards in the tuning sample: every board of small batches, every k-th of large ones.
+constexpr uint64_t kTuneSample = 4096;
+
+// Times every (block, split factor) candidate once on a stride sample of the boards: the
+// sample's own schedule and one launch each, timed with CUDA events.  Each board stands for
+// its subtree, so the sample keeps the batch's spread of sizes at 1/stride of its work.
+int tune_on_sample(nqb_batch_plan* p, const nqb_opts& o, const std::vector<int>& blocks,
+                   const std::vector<int>& factors, int* best_block, int* best_factor) {
+    const uint64_t stride = std::max<uint64_t>(1, p->count / kTuneSample);
+    const uint64_t n = (p->count + stride - 1) / stride;
+    nqb_state* d_sample = nullptr;
+    unsigned long long* d_split = nullptr;
+    int st = nqb::dev_alloc(&d_sample, n * sizeof(nqb_state), p->s);
+    if (!st) st = nqb::dev_alloc(&d_split, sizeof(unsigned long long), p->s);
+    if (!st) {
+        stride_gather<<<(unsigned)((n + 255) / 256), 256, 0, p->s>>>(reinterpret_cast<const uint4*>(p->d_boards), n,
+                                                                      stride, reinterpret_cast<uint4*>(d_sample));
+        st = cuda_status(cudaGetLastError());
+    }
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (!st) st = cuda_status(cudaEventCreate(&a));
+    if (!st) st = cuda_status(cudaEventCreate(&b));
+    float best = -1.0f;
+    for (size_t fi = 0; fi < factors.size() && !st; ++fi) {
+        nqb_opts oo = o;
+        oo.split_factor = factors[fi];
+        nqb::Schedule sch;
+        st = nqb::schedule_items(d_sample, (uint32_t)n, nullptr, oo, p->device, p->s, d_split, nullptr, &sch);
+        for (size_t bi = 0; bi < blocks.size() && !st; ++bi) {
+            st = cuda_status(
+                cudaMemsetAsync(p->d_out, 0, 8 * sizeof(unsigned long long) + nqb::kBatchedScratchBytes, p->s));
+            if (!st) st = cuda_status(cudaEventRecord(a, p->s));
+            if (!st)
+                st = nqb::launch_batched(reinterpret_cast<const nqb_state*>(sch.items), sch.n, sch.order, sch.board,
+                                         p->d_out + 8, nqb::kBatchedScratchBytes, p->d_out, nullptr, nullptr,
+                                         blocks[bi], p->stack_depth, p->device, p->s, nullptr);
+            if (!st) st = cuda_status(cudaEventRecord(b, p->s));
+            if (!st) st = cuda_status(cudaEventSynchronize(b));
+            float ms = 0.0f;
+            if (!st) st = cuda_status(cudaEventElapsedTime(&ms, a, b));
+            if (!st && (best < 0.0f || ms < best)) {
+                best = ms;
+                *best_block = blocks[bi];
+                *best_factor = factors[fi];
+            }
+        }
+        sch.release();
+    }
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    nqb::dev_free(d_sample, p->s);
+    nqb::dev_free(d_split, p->s);
+    if (!st) st = cuda_status(cudaStreamSynchronize(p->s));
+    return st;
+}
+
 }  // namespace
 
 extern "C" {
@@ -148,7 +213,8 @@ int nqb_batch_plan_create(const nqb_state* boards, uint64_t count, const nqb_opt
     if ((st = cuda_status(cudaStreamCreateWithFlags(&p->s, cudaStreamNonBlocking)))) return fail(st);
     if ((st = cuda_status(cudaMalloc(&p->d_boards, count * sizeof(nqb_state))))) return fail(st);
     if ((st = cuda_status(cudaMalloc(&p->d_per, count * sizeof(unsigned long long))))) return fail(st);
-    if ((st = cuda_status(cudaMalloc(&p->d_out, 5 * sizeof(unsigned long long))))) return fail(st);
+    if ((st = cuda_status(cudaMalloc(&p->d_out, 8 * sizeof(unsigned long long) + nqb::kBatchedScratchBytes))))
+        return fail(st);
     if ((st = cuda_status(cudaMalloc(&p->d_split, sizeof(unsigned long long))))) return fail(st);
     if ((st = cuda_status(cudaMallocHost(&p->h_per, count * sizeof(unsigned long long))))) return fail(st);
     if ((st = cuda_status(cudaMallocHost(&p->h_out, 4 * sizeof(unsigned long long))))) return fail(st);
@@ -159,43 +225,17 @@ int nqb_batch_plan_create(const nqb_state* boards, uint64_t count, const nqb_opt
     std::vector<int> blocks, factors;
     if (autotune) {
         blocks = {64, 128, 256};
-        factors = o.model ? std::vector<int>{1, 4, 16} : std::vector<int>{o.split_factor};
+        factors = (o.model || o.sched_cost) ? std::vector<int>{1, 4, 16} : std::vector<int>{o.split_factor};
     } else {
         blocks = {o.block_size ? o.block_size : 128};
         factors = {o.split_factor};
     }
-    const bool timed = blocks.size() * factors.size() > 1;
-    float best = 0.0f;
     int best_block = blocks[0], best_factor = factors[0];
-    for (int f : factors) {
-        if ((st = build_schedule(p, o, f))) return fail(st);
-        for (int b : blocks) {
-            cudaGraphExec_t ex = nullptr;
-            if ((st = capture(p, b, &ex))) return fail(st);
-            float ms = 0.0f;
-            if (timed && (st = time_graph(p, ex, &ms))) {
-                cudaGraphExecDestroy(ex);
-                return fail(st);
-            }
-            if (!p->exec || ms < best) {
-                if (p->exec) cudaGraphExecDestroy(p->exec);
-                p->exec = ex;
-                best = ms;
-                best_block = b;
-                best_factor = f;
-            } else {
-                cudaGraphExecDestroy(ex);
-            }
-        }
-    }
-    // a kept graph reads the schedule of its own split factor: rebuild both if another
-    // factor was tried after the winner
-    if (best_factor != p->factor) {
-        cudaGraphExecDestroy(p->exec);
-        p->exec = nullptr;
-        if ((st = build_schedule(p, o, best_factor))) return fail(st);
-        if ((st = capture(p, best_block, &p->exec))) return fail(st);
-    }
+    if (blocks.size() * factors.size() > 1 &&
+        (st = tune_on_sample(p, o, blocks, factors, &best_block, &best_factor)))
+        return fail(st);
+    if ((st = build_schedule(p, o, best_factor))) return fail(st);
+    if ((st = capture(p, best_block, &p->exec))) return fail(st);
     p->block = best_block;
     *out = p;
     cudaSetDevice(p->prev_device);
@@ -211,7 +251,7 @@ int nqb_batch_plan_run(nqb_batch_plan* p, uint64_t* out, nqb_stats* stats) {
     if (!st) st = time_graph(p, p->exec, &ms);
     if (!st) {
         std::memcpy(out, p->h_per, p->count * sizeof(uint64_t));
-        if (p->h_out[3]) st = NQB_E_DEVICE;
+        if (p->h_out[3]) st = (p->h_out[3] & 4) ? NQB_E_STALL : NQB_E_DEVICE;
     }
     if (!st && stats) {
         std::memset(stats, 0, sizeof(*stats));

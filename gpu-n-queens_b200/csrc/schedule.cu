@@ -13,7 +13,9 @@
 //      to max_split_rounds rounds or until nothing is split;
 //   3. order the queue by predicted cost, largest first (CUB radix sort of (cost, index));
 //   4. one launch of the batched kernel with that order.
-// Without a model the items go to the kernel unchanged, in their given order (FIFO).
+// Without a model the items go to the kernel unchanged, in their given order (FIFO), unless
+// a model-free cost is asked for (nqb_opts.sched_cost: the ablation arms of the learned
+// schedule), which then drives the same split-and-order steps in place of the prediction.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -114,6 +116,25 @@ __global__ void split_kernel(const uint4* __restrict__ items, const uint32_t* __
     if (board_nodes) atomicAdd(board_nodes + b_id, (unsigned long long)placed);
 }
 
+// Model-free costs (log2 of an estimate of the nodes below each item), the ablation arms of
+// the learned schedule: kind 1 = free columns x rows left; kind 2 = the product over the rows
+// below of (1 + the cells the queens above leave free in that row).
+__global__ void heuristic_cost_kernel(const uint4* __restrict__ items, uint32_t n, int kind, float* __restrict__ cost) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint4 s = items[i];
+    uint32_t nc;
+    item_avail(s, &nc);
+    const uint32_t rows_left = ((s.w >> 8) & 0xFFu) - (s.w & 0xFFu);
+    if (kind == 1) {
+        cost[i] = log2f(1.0f + (float)__popc(nc) * (float)rows_left);
+        return;
+    }
+    float c = 0.0f;
+    for (uint32_t k = 0; k < rows_left && k < 32; ++k) c += log2f(1.0f + (float)__popc(nc & ~((s.y << k) | (s.z >> k))));
+    cost[i] = c;
+}
+
 }  // namespace
 
 int schedule_items(const nqb_state* d_items, uint32_t n, const uint32_t* d_board, const nqb_opts& o, int device,
@@ -124,8 +145,10 @@ int schedule_items(const nqb_state* d_items, uint32_t n, const uint32_t* d_board
     out->order = nullptr;
     out->n = n;
     out->sched_ms = 0.0;
-    if (!o.model) return NQB_OK;
-    if (model_device(o.model) != device) return NQB_E_INVALID;
+    const int heuristic = o.model ? 0 : o.sched_cost;  // a model takes precedence
+    if (!o.model && heuristic == 0) return NQB_OK;
+    if (heuristic < 0 || heuristic > 2) return NQB_E_INVALID;
+    if (o.model && model_device(o.model) != device) return NQB_E_INVALID;
     const int rounds = o.max_split_rounds < 0 ? 3 : o.max_split_rounds;
     const int factor = o.split_factor > 0 ? o.split_factor : 4;
     int sms = 0;
@@ -161,7 +184,13 @@ int schedule_items(const nqb_state* d_items, uint32_t n, const uint32_t* d_board
     if (st) return st;
     for (int r = 0;; ++r) {
         if ((st = cost.alloc(n))) return st;
-        if ((st = model_predict_device(o.model, reinterpret_cast<const nqb_state*>(cur_items), n, cost.p, s))) return st;
+        if (heuristic) {
+            heuristic_cost_kernel<<<(n + 255) / 256, 256, 0, s>>>(cur_items, n, heuristic, cost.p);
+            if ((st = cuda_status(cudaGetLastError()))) return st;
+        } else if ((st = model_predict_device(o.model, reinterpret_cast<const nqb_state*>(cur_items), n, cost.p,
+                                              s))) {
+            return st;
+        }
         if (r >= rounds) break;
         cudaMemsetAsync(work.p, 0, sizeof(double), s);
         work_sum_kernel<<<std::max(1u, std::min((n + 255) / 256, 1024u)), 256, 0, s>>>(cost.p, n, work.p);
@@ -227,15 +256,17 @@ void Schedule::release() {
 
 // Runs the batched form on `n` device items.  `d_board` (optional) maps items to output
 // slots.  Extra nodes made by splitting are added into d_out[1] (and d_per_board_nodes).
-int launch_batched_scheduled(const nqb_state* d_items, uint32_t n, const uint32_t* d_board, uint32_t* d_head,
-                             unsigned long long* d_out, unsigned long long* d_per_board,
+int launch_batched_scheduled(const nqb_state* d_items, uint32_t n, const uint32_t* d_board, void* d_scratch,
+                             size_t scratch_bytes, unsigned long long* d_out, unsigned long long* d_per_board,
                              unsigned long long* d_per_board_nodes, const nqb_opts& o, unsigned stack_depth,
-                             int device, cudaStream_t s, unsigned* launches, SchedInfo* info) {
+                             int device, cudaStream_t s, unsigned* launches, SchedInfo* info,
+                             unsigned long long* d_lane_stats) {
     Schedule sch;
     int st = schedule_items(d_items, n, d_board, o, device, s, d_out + 1, d_per_board_nodes, &sch);
     if (!st)
-        st = launch_batched(reinterpret_cast<const nqb_state*>(sch.items), sch.n, sch.order, sch.board, d_head, d_out,
-                            d_per_board, d_per_board_nodes, o.block_size, stack_depth, device, s, launches);
+        st = launch_batched(reinterpret_cast<const nqb_state*>(sch.items), sch.n, sch.order, sch.board, d_scratch,
+                            scratch_bytes, d_out, d_per_board, d_per_board_nodes, o.block_size, stack_depth, device,
+                            s, launches, d_lane_stats);
     sch.release();  // stream-ordered after the kernel that reads the arrays
     if (info) {
         info->items = sch.n;

@@ -36,13 +36,13 @@ int time_candidate(const nqb_state* d_sample, uint32_t count, unsigned depth, co
     int st = cuda_status(cudaEventCreate(&e1));
     double best = -1.0;
     for (int rep = 0; rep < 2 && !st; ++rep) {
-        st = cuda_status(cudaMemsetAsync(d_out, 0, 5 * sizeof(unsigned long long), s));
+        st = cuda_status(cudaMemsetAsync(d_out, 0, 8 * sizeof(unsigned long long) + kBatchedScratchBytes, s));
         if (!st) st = cuda_status(cudaEventRecord(e0, s));
         unsigned launches = 0;
         if (!st) {
             if (c.form == NQB_FORM_BATCHED) {
                 SchedInfo info;
-                st = launch_batched_scheduled(d_sample, count, nullptr, reinterpret_cast<uint32_t*>(d_out + 4), d_out,
+                st = launch_batched_scheduled(d_sample, count, nullptr, d_out + 8, kBatchedScratchBytes, d_out,
                                               nullptr, nullptr, o, depth, device, s, &launches, &info);
             } else {
                 st = launch_plain(d_sample, count, d_out, nullptr, c.block, false, depth, s, &launches);
@@ -54,7 +54,7 @@ int time_candidate(const nqb_state* d_sample, uint32_t count, unsigned depth, co
         if (!st) st = cuda_status(cudaStreamSynchronize(s));
         float t = 0.0f;
         if (!st) st = cuda_status(cudaEventElapsedTime(&t, e0, e1));
-        if (!st && h[3]) st = NQB_E_DEVICE;
+        if (!st && h[3]) st = (h[3] & 4) ? NQB_E_STALL : NQB_E_DEVICE;
         if (!st) {
             if (best < 0 || t < best) best = t;
             *sample_count = h[0];
@@ -87,12 +87,12 @@ extern "C" int nqb_tune_count(unsigned n, const unsigned* depths, unsigned n_dep
     cudaStream_t s = nullptr;
     if (!st) st = cuda_status(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     unsigned long long* d_out = nullptr;
-    if (!st) st = dev_alloc(&d_out, 5 * sizeof(unsigned long long), s);
+    if (!st) st = dev_alloc(&d_out, 8 * sizeof(unsigned long long) + kBatchedScratchBytes, s);  // results, scratch
 
     std::vector<Candidate> cands;
     for (int form : {NQB_FORM_PLAIN, NQB_FORM_BATCHED})
         for (int block : {64, 128, 256}) {
-            if (form == NQB_FORM_BATCHED && base.model) {
+            if (form == NQB_FORM_BATCHED && (base.model || base.sched_cost)) {
                 for (int factor : {1, 4, 16}) cands.push_back({form, block, factor});
             } else {
                 cands.push_back({form, block, 0});

@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define NQB_VERSION 10000 /* 1.0.0 */
+#define NQB_VERSION 10100 /* 1.1.0 */
 
 /* Board sizes.  The reference accepts 7 < N < 32 (deffinitions.cuh:116-118);
  * this library accepts 4..31.  Counts are exact in uint64 up to N = 28. */
@@ -93,7 +93,14 @@ typedef struct nqb_opts {
                              the GPU (the reference's way); 0 = build it on the GPU    */
     int autotune;         /* nqb_count_ex: 1 = pick form, block size and split factor with
                              nqb_tune_count on a 1/64 sample of the pool first          */
-    int reserved[6];
+    int count_lane_steps; /* 1: run the instrumented search kernel that also counts its
+                             lane-steps (nqb_stats.placed_lane_steps, lane_step_slots)  */
+    int sched_cost;       /* batched form without a model: 0 = FIFO; a model-free cost drives
+                             the learned schedule's split-and-order steps instead of the
+                             network (its ablation): 1 = log2(1 + free columns x rows
+                             left), 2 = sum over the rows below of log2(1 + cells left
+                             free there by the queens above)                           */
+    int reserved[4];
 } nqb_opts;
 
 typedef struct nqb_stats {
@@ -110,6 +117,11 @@ typedef struct nqb_stats {
     double sched_ms;     /* learned scheduling: prediction, splitting, ordering        */
     uint32_t block_size; /* threads per block of the search launch                        */
     int32_t form;        /* search form used (NQB_FORM_*)                                  */
+    /* With nqb_opts.count_lane_steps (else 0): lane-steps of the search loop that placed a
+     * queen, and lane-step slots issued (32 per warp step).  Their ratio is the search's
+     * warp execution efficiency in active lanes. */
+    uint64_t placed_lane_steps;
+    uint64_t lane_step_slots;
 } nqb_stats;
 
 /* Fills `opts` with the defaults (device 0, plain form, library block size). */
@@ -382,6 +394,28 @@ int nqb_plain_launch(const nqb_state* d_states, uint64_t count, uint64_t* d_out,
 int nqb_batched_launch(const nqb_state* d_items, uint64_t count, const uint32_t* d_order, uint32_t* d_head,
                        uint64_t* d_out, int block_size, unsigned stack_depth, void* stream);
 
+/* Scratch of nqb_batched_launch_ex with the library's own steal ring (65,536 slots). */
+#define NQB_BATCHED_SCRATCH_BYTES (64ull + 32ull * 65536ull)
+
+/*
+ * The batched form with work stealing across warps.  d_scratch (16-byte aligned, zeroed
+ * before every launch) holds 64 bytes of control words and a ring of 32-byte slots:
+ * warps that run out of work take rows from the ring, and while such warps exist the
+ * other warps publish their lanes' shallowest pending rows into it, so a long subtree
+ * spreads over the whole GPU.  The ring uses the largest power of two of slots that fits
+ * (NQB_BATCHED_SCRATCH_BYTES: 65,536); scratch_bytes below 64 + 2 x 32 launches without
+ * the ring, exactly as nqb_batched_launch.  d_lane_stats (optional): two device uint64
+ * words, zeroed first, that the instrumented kernel adds {lane-steps that placed a queen,
+ * lane-step slots} into.  wait_limit: polls without progress after which a waiting warp
+ * gives up (0 = the library default, about 2 s); a launch in which one gave up sets error
+ * flag 4 in d_out[3] (NQB_E_STALL from the calls that read it) and its counts are not to
+ * be used.  count <= 2^31.  Asynchronous.  Extends the kernel launch of gpu_solver_driver
+ * (GPU_NQueens.cu:128-138), which has no work sharing.
+ */
+int nqb_batched_launch_ex(const nqb_state* d_items, uint64_t count, const uint32_t* d_order, void* d_scratch,
+                          uint64_t scratch_bytes, uint64_t* d_out, uint64_t* d_lane_stats, int block_size,
+                          unsigned stack_depth, unsigned wait_limit, void* stream);
+
 /* ---- learned cost model ------------------------------------------------ */
 /*
  * An MLP (NQB_MODEL_INPUTS -> 128 -> 128 -> 1, GELU) predicting log2(1 + nodes) of the
@@ -416,9 +450,12 @@ int nqb_model_features(const nqb_state* states, uint64_t count, float* features)
 int nqb_model_predict(const nqb_model* model, const nqb_state* states, uint64_t count, float* log2_nodes);
 /* Same, with an explicit bound on the wait for each tensor-core product: `wait_limit`
  * non-blocking probes of its completion barrier (0 = the library's default bounded wait).
- * A wait that runs out drains the products in flight, frees the block's tensor memory and
- * makes the call return NQB_E_STALL with `log2_nodes` undefined; the model and the device
- * stay usable.  A bound of 1 forces that path (tests). */
+ * A wait that runs out drains the products in flight (a second bounded wait), frees the
+ * block's tensor memory and makes the call return NQB_E_STALL with `log2_nodes` undefined;
+ * the model and the device stay usable.  If the drain runs out as well, products may still
+ * have been writing the tensor memory when it was freed: the call returns NQB_E_DEVICE, and
+ * later results on that device are not to be trusted.  A bound of 1 forces the first path
+ * (tests); the default drain bound is seconds. */
 int nqb_model_predict_ex(const nqb_model* model, const nqb_state* states, uint64_t count, float* log2_nodes,
                          uint32_t wait_limit);
 /* One forward and backward pass over all `count` rows (count <= 2^20): mean squared
@@ -436,11 +473,13 @@ int nqb_record_nodes(const nqb_state* states, uint64_t count, const nqb_opts* op
 /* ---- batch plans: one board set solved repeatedly through a CUDA graph --- */
 /*
  * A plan uploads `count` boards once, builds the batched form's schedule (with
- * opts->model: learned splitting and largest-first order) and captures the solve
- * (zeroing of the outputs, one persistent-kernel launch, read-back) into a CUDA graph.
- * With autotune != 0 every candidate (block size 64/128/256 x split factor 1/4/16 when a
- * model is given) is captured and timed once on the GPU and the fastest is kept.  The
- * model is only read during creation.  No counterpart in the reference.
+ * opts->model, or a model-free opts->sched_cost: splitting and largest-first order) and
+ * captures the solve (zeroing of the outputs and the launch scratch, one persistent-kernel
+ * launch with work stealing, read-back) into a CUDA graph.  With autotune != 0 every
+ * candidate (block size 64/128/256 x split factor 1/4/16 when a cost is given) is first
+ * timed once on a stride sample of about 4,096 boards, and the fastest is captured for
+ * the whole batch.  The model is only read during creation.  No counterpart in the
+ * reference.
  */
 typedef struct nqb_batch_plan nqb_batch_plan;
 int nqb_batch_plan_create(const nqb_state* boards, uint64_t count, const nqb_opts* opts, int autotune,
@@ -460,19 +499,22 @@ void nqb_batch_plan_destroy(nqb_batch_plan* plan);
  * nqb_batched_launch for callers that cannot allocate device memory.  It has no
  * counterpart in the reference.
  *
- * Some callers may not call cudaMalloc or cudaFree at all: code running inside a
- * stream capture (allocation is not a capturable operation), code whose framework
- * hands out all device memory through its own caching allocator, and code that must
- * not stall the GPU (cudaFree synchronises the device).  This entry point needs no
- * scratch buffer from them: the queue head lives in a 256-byte array of this library's
- * device memory (NQB_STATIC_SCRATCH_BYTES), which every GPU that loads the library
- * holds until the process exits.  The caller still passes the items, the optional
- * order and the four result words, exactly as for nqb_batched_launch; this call
- * allocates nothing and calls no allocating library routine.
+ * Some callers may not call cudaMalloc or cudaFree at all: code whose framework hands
+ * out all device memory through its own caching allocator (a raw cudaMalloc beside it
+ * fragments or oversubscribes what the framework budgets), and code that must not stall
+ * the GPU (cudaFree synchronises the whole device).  This entry point needs no scratch
+ * buffer from them: the queue head lives in a 256-byte array of this library's device
+ * memory (NQB_STATIC_SCRATCH_BYTES), which every GPU that loads the library holds until
+ * the process exits.  The caller still passes the items, the optional order and the four
+ * result words, exactly as for nqb_batched_launch; this call allocates nothing and calls
+ * no allocating library routine.  It launches without the steal ring of
+ * nqb_batched_launch_ex (warps share work only inside themselves).
  *
  * - The first call on a device looks the array's device address up
  *   (cudaGetSymbolAddress) with that device current; make that first call before any
- *   stream capture on the device.
+ *   stream capture on the device.  The address is kept per device and context: after a
+ *   device reset (cudaDeviceReset) the next call looks it up again, so that call is a
+ *   first call too.
  * - Each call clears the queue head on `stream` before launching (the array keeps
  *   whatever the previous call left).  All calls on a device share the one array, so
  *   calls whose work overlaps on the GPU race: serialise them, e.g. on one stream.

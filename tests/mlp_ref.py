@@ -28,23 +28,37 @@ def gelu_grad(x):
 
 
 def features(states):
-    """Same encoding as the library: free-column, ldiag, rdiag bits, then 4 scalars."""
+    """Same encoding as the library (board-relative): free cells of each of the next 32 rows,
+    the free-column and candidate masks centred on the board, then 6 scalars."""
     st = np.asarray(states)
-    n = st["n"].astype(np.uint64)
-    mask = ((np.uint64(1) << n) - np.uint64(1)).astype(np.uint64)
+    n = st["n"].astype(np.int64)
+    row = st["row"].astype(np.int64)
+    mask = ((np.int64(1) << n) - 1).astype(np.uint64)
     cols, ld, rd = (st[k].astype(np.uint64) for k in ("cols", "ldiag", "rdiag"))
-    nc = mask & ~cols & np.uint64(0xFFFFFFFF)
-    avail = nc & ~(ld | rd)
+    m32 = np.uint64(0xFFFFFFFF)
+    nc = mask & ~cols & m32
+    avail = nc & ~(ld | rd) & m32
+    left = np.maximum(n - row, 0)
+    shift = (16 - (n >> 1)).astype(np.uint64)
+    pc = np.vectorize(lambda v: bin(int(v)).count("1"), otypes=[np.int64])
     X = np.zeros((len(st), IN), dtype=np.float64)
+    if not len(st):
+        return X
+    look = np.zeros((len(st), 32), dtype=np.int64)
+    for k in range(32):
+        kk = np.uint64(k)
+        cells = pc(nc & ~(((ld << kk) & m32) | (rd >> kk)))
+        look[:, k] = np.where(k < left, cells, 0)
+    X[:, 0:32] = look / 32.0
     bits = np.arange(32, dtype=np.uint64)
-    X[:, 0:32] = (nc[:, None] >> bits) & np.uint64(1)
-    X[:, 32:64] = ((ld & mask)[:, None] >> bits) & np.uint64(1)
-    X[:, 64:96] = (rd[:, None] >> bits) & np.uint64(1)
-    pc = np.vectorize(lambda v: bin(int(v)).count("1"))
-    X[:, 96] = n / 32.0
-    X[:, 97] = st["row"] / 32.0
-    X[:, 98] = pc(nc) / 32.0 if len(st) else 0
-    X[:, 99] = pc(avail) / 32.0 if len(st) else 0
+    X[:, 32:64] = ((((nc << shift) & m32)[:, None]) >> bits) & np.uint64(1)
+    X[:, 64:96] = ((((avail << shift) & m32)[:, None]) >> bits) & np.uint64(1)
+    X[:, 96] = left / 32.0
+    X[:, 97] = pc(nc) / 32.0
+    X[:, 98] = pc(avail) / 32.0
+    X[:, 99] = n / 32.0
+    X[:, 100] = row / 32.0
+    X[:, 101] = look.sum(1) / 256.0
     return X
 
 

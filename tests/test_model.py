@@ -124,17 +124,27 @@ def test_learned_schedule_per_board(nqb, nqo, trained):
 
 
 @pytest.mark.gpu
-def test_learned_schedule_beats_fifo_on_coarse_pool(nqb, trained):
-    """Ablation: what the trained model gains over the same batched kernel with FIFO order.
-    N=17 with a depth-3 pool has 1,473 items for ~150k resident lanes; FIFO leaves most lanes
-    without work, the learned schedule splits the items predicted largest and orders the
-    queue largest first (B200: ~190 ms -> ~10 ms)."""
-    for _ in range(2):  # the second round is the measured one
-        c_f, st_f = nqb.count_ex(17, 3, form=1)
-        c_l, st_l = nqb.count_ex(17, 3, form=1, model=trained)
-    assert c_f == c_l == KAT[17] and st_f["nodes"] == st_l["nodes"]
-    assert st_l["items"] > st_f["items"]
-    assert st_l["kernel_ms"] < 0.5 * st_f["kernel_ms"], (st_l, st_f)
+def test_schedule_ablation_arms_are_exact(nqb, trained):
+    """Ablation of the learned schedule: the same split-and-order pipeline driven by the trained
+    network, an untrained one and the two model-free costs, against FIFO with work stealing.
+    N=17 with a depth-3 pool has 1,473 items for ~150k resident lanes.  Every arm must be
+    exact; the arms' speeds are measured by the bench (extras.ablation), and here the trained
+    arm must at least not lose to the untrained network by more than noise."""
+    untrained = nqb.Model(seed=5)
+    try:
+        arms = {"fifo": {}, "untrained": {"model": untrained}, "free_x_rows": {"sched_cost": 1},
+                "lookahead": {"sched_cost": 2}, "trained": {"model": trained}}
+        ms = {}
+        for name, kw in arms.items():
+            for _ in range(2):  # the second run is the measured one
+                c, st = nqb.count_ex(17, 3, form=1, **kw)
+            assert c == KAT[17], name
+            ms[name] = st["kernel_ms"]
+            if name != "fifo":
+                assert st["items"] > 1473, name
+        assert ms["trained"] < 1.5 * ms["untrained"] + 5.0, ms
+    finally:
+        untrained.close()
 
 
 @pytest.mark.gpu

@@ -1,6 +1,6 @@
 """nqb_batched_launch_static: the batched launch for callers that cannot allocate device
-memory (inside a stream capture, under a framework's caching allocator, or where cudaFree's
-device-wide synchronisation is not allowed).  Its queue head lives in the library's own
+memory (under a framework's caching allocator, or where cudaFree's device-wide
+synchronisation is not allowed).  Its queue head lives in the library's own
 256-byte device array, so the caller passes only the items and the result words.
 
 Checked through the C ABI against nqb_batched_launch (the entry point that takes a
