@@ -11,6 +11,11 @@
 //   ref_harness writemix <d1> <d2> <file>        the d1 and d2 pools interleaved state by state,
 //                                                written by util_write_nq_states_to_stream
 //   ref_harness readfile <file>                  util_read_nq_states_from_stream: count, lock, hash
+//   ref_harness boards <file> <threads>          partial boards of this N, one per line "d c0 .. c(d-1)":
+//                                                each built with init_nq_state + place_queen_at and
+//                                                streamed with locked_advance_nq_state(d, N-1)
+//                                                (n_queens.cu:423-445), no mirror weight: the
+//                                                completions and placements below row d of each
 #include "deffinitions.cuh"
 #undef N
 #define N NQO_REF_N
@@ -216,6 +221,56 @@ static int cmd_readfile(const char* path) {
     return 0;
 }
 
+static int cmd_boards(const char* path, unsigned threads) {
+    FILE* f = fopen(path, "r");
+    if (!f) return 3;
+    std::vector<nq_state_t> boards;
+    std::vector<unsigned> depth;
+    char line[512];
+    while (fgets(line, sizeof line, f)) {
+        char* p = line;
+        char* e = nullptr;
+        const unsigned d = (unsigned)strtoul(p, &e, 10);
+        if (e == p) continue;
+        p = e;
+        nq_state_t s = init_nq_state();
+        for (unsigned r = 0; r < d; ++r) {
+            const unsigned c = (unsigned)strtoul(p, &e, 10);
+            p = e;
+            place_queen_at(&s, (unsigned char)r, (unsigned char)c);
+        }
+        s.curr_row = (char)d;
+        boards.push_back(s);
+        depth.push_back(d);
+    }
+    fclose(f);
+    std::vector<uint64_t> count(boards.size()), nodes(boards.size());
+    std::atomic<uint64_t> next(0);
+    auto work = [&]() {
+        for (;;) {
+            const uint64_t k = next.fetch_add(1);
+            if (k >= boards.size()) break;
+            nq_state_t s = boards[k];
+            uint64_t c = 0, ln = 0;
+            while (locked_advance_nq_state(&s, depth[k], N - 1)) {
+                ln++;
+                c += (s.queens_in_columns == N_MASK);
+            }
+            count[k] = c;
+            nodes[k] = ln;
+        }
+    };
+    std::vector<std::thread> ts;
+    for (unsigned t = 0; t < (threads ? threads : 1); ++t) ts.emplace_back(work);
+    for (auto& t : ts) t.join();
+    printf("NQO_JSON {\"n\": %u, \"boards\": %zu, \"count\": [", (unsigned)N, boards.size());
+    for (size_t i = 0; i < boards.size(); ++i) printf("%s%" PRIu64, i ? ", " : "", count[i]);
+    printf("], \"nodes\": [");
+    for (size_t i = 0; i < boards.size(); ++i) printf("%s%" PRIu64, i ? ", " : "", nodes[i]);
+    printf("]}\n");
+    return 0;
+}
+
 int main(int argc, char** argv) {
     if (argc < 3) {
         fprintf(stderr, "usage: %s pool|dump|replay|cpu|gpu <d> ...\n", argv[0]);
@@ -238,6 +293,8 @@ int main(int argc, char** argv) {
     if (!strcmp(argv[1], "writemix") && argc > 4)
         return cmd_writemix(d, (unsigned)strtoul(argv[3], nullptr, 10), argv[4]);
     if (!strcmp(argv[1], "readfile")) return cmd_readfile(argv[2]);
+    if (!strcmp(argv[1], "boards"))
+        return cmd_boards(argv[2], argc > 3 ? (unsigned)strtoul(argv[3], nullptr, 10) : 1);
     if (!strcmp(argv[1], "gpu")) return cmd_gpu(d, argc > 3 ? (unsigned)strtoul(argv[3], nullptr, 10) : 1);
     fprintf(stderr, "unknown command\n");
     return 1;
