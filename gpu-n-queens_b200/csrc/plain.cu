@@ -17,8 +17,8 @@ namespace nqb {
 namespace {
 
 constexpr unsigned kFull = 0xFFFFFFFFu;
-constexpr int kUnroll = 16;
-constexpr uint32_t kEpoch = 1u << 22;  // votes between folds: 31 nodes x kUnroll x kEpoch < 2^32
+constexpr int kUnroll = 64;  // steps between done-votes (16 and 32 measured 0.6% slower)
+constexpr uint32_t kEpoch = (1u << 27) / kUnroll;  // votes between folds: 31 nodes x kUnroll x kEpoch < 2^32
 
 // Error flags written to out[3].
 constexpr unsigned kErrStack = 1u;  // a state needed a deeper stack than provided

@@ -14,7 +14,8 @@
 // consecutive 16-byte slots and an LDS.128 / STS.128 needs no bank replays.
 //
 // Per step: if the row has no candidate left, pop the deepest pending row; place the
-// lowest candidate b; push the row back only if candidates remain; step to the next
+// lowest candidate b (avail & (avail - 1) is the row without it, and their XOR is b); push
+// the row back only if candidates remain; step to the next
 // row and "enter" it.  A row left without candidates is not pushed, so a row with one
 // free column is filled without creating a branch point: the reference's unit-row
 // propagation (GPU_NQueens.cu:392-408, n_queens.cuh:145-163).  b is a free column, so it
@@ -138,10 +139,11 @@ __device__ __forceinline__ StepInfo search_step(Lane& s, uint32_t base, uint32_t
         "@p ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n\t"
         "setp.ne.and.u32 q, %4, %9, p;\n\t"
         "@q sub.u32 %4, %4, %10;\n\t"
-        "neg.s32 x, %0;\n\t"                               // b = lowest candidate
-        "and.b32 %7, %0, x;\n\t"
-        "sub.u32 %0, %0, %7;\n\t"
-        "setp.ne.u32 t, %0, 0;\n\t"                        // candidates remain: push the row
+        "sub.u32 x, %0, 1;\n\t"                            // the row without its lowest candidate b
+        "and.b32 x, x, %0;\n\t"
+        "setp.ne.u32 t, x, 0;\n\t"                         // candidates remain: push the row
+        "xor.b32 %7, %0, x;\n\t"
+        "mov.u32 %0, x;\n\t"
         "@t add.u32 %4, %4, %10;\n\t"
         "@t st.shared.v4.u32 [%4], {%0, %1, %2, %3};\n\t"
         "sub.u32 %1, %1, %7;\n\t"                          // next row
@@ -162,10 +164,11 @@ __device__ __forceinline__ StepInfo search_step(Lane& s, uint32_t base, uint32_t
         "@p ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n\t"
         "setp.ne.and.u32 q, %4, %10, p;\n\t"
         "@q sub.u32 %4, %4, %11;\n\t"
-        "neg.s32 x, %0;\n\t"
-        "and.b32 %7, %0, x;\n\t"
-        "sub.u32 %0, %0, %7;\n\t"
-        "setp.ne.u32 t, %0, 0;\n\t"
+        "sub.u32 x, %0, 1;\n\t"
+        "and.b32 x, x, %0;\n\t"
+        "setp.ne.u32 t, x, 0;\n\t"
+        "xor.b32 %7, %0, x;\n\t"
+        "mov.u32 %0, x;\n\t"
         "add.u32 nsp, %4, %11;\n\t"                        // the push's slot must not pass top
         "setp.gt.u32 ov, nsp, %12;\n\t"
         "and.pred ok, t, !ov;\n\t"
