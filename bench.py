@@ -412,9 +412,25 @@ def run_extras(nqb, dev, args):
     pp = model.predict(pool).astype(np.float64)
     out["model"]["n19_d5_pool"] = {"items": len(pool), "rmse_log2": round(float(np.sqrt(np.mean((pp - pt) ** 2))), 4),
                                    "std_log2": round(float(np.std(pt)), 4), "spearman": round(_spearman(pp, pt), 4)}
+    # the same network trained on mixed board sizes (n 16..20, depth 4..8), reported beside it
+    mb = nqb.sample_boards(nqb.MODEL_SEED, args.model_samples, 16, 20, 4, 8)
+    mn, _ = nqb.record_nodes(mb, device=dev)
+    mt = np.log2(1.0 + mn.astype(np.float64)).astype(np.float32)
+    mixed = nqb.Model(device=dev, seed=1)
+    mixed.train(mb[:ntr], mt[:ntr], epochs=8, batch=4096, lr=2e-3)
+    mp = mixed.predict(mb[ntr:])
+    qp = mixed.predict(pool).astype(np.float64)
+    out["model_mixed_n"] = {"train_set": "n=16..20, depth 4..8 (seeded sampler)", "samples": len(mb),
+                            "val_rmse_log2": round(float(np.sqrt(np.mean((mp - mt[ntr:]) ** 2))), 4),
+                            "val_std_log2": round(float(np.std(mt[ntr:])), 4),
+                            "val_spearman": round(_spearman(mp, mt[ntr:]), 4),
+                            "n19_d5_pool": {"rmse_log2": round(float(np.sqrt(np.mean((qp - pt) ** 2))), 4),
+                                            "std_log2": round(float(np.std(pt)), 4),
+                                            "spearman": round(_spearman(qp, pt), 4)}}
     untrained = nqb.Model(device=dev, seed=1)
     arms = {"fifo": {}, "untrained_net": {"model": untrained}, "free_x_rows": {"sched_cost": 1},
-            "lookahead_cells": {"sched_cost": 2}, "trained_net": {"model": model}}
+            "lookahead_cells": {"sched_cost": 2}, "trained_net": {"model": model},
+            "trained_mixed_n": {"model": mixed}}
 
     # the ablation on coarse full counts: kernel + scheduling time of each arm (second of two runs)
     abl = {}
@@ -467,6 +483,7 @@ def run_extras(nqb, dev, args):
                         "learned_items": s2["items"], "learned_over_plain": round(s0["kernel_ms"] / s2["kernel_ms"], 3)}
     out["n19"] = n19
     untrained.close()
+    mixed.close()
     model.close()
     return out
 

@@ -14,7 +14,8 @@
 //   - stealing across warps (when the launch has a steal ring): a warp with no work left
 //     registers as hungry and takes rows from a device ring; while hungry warps exist,
 //     busy warps publish the shallowest pending rows of their lanes into it, so a long
-//     subtree spreads over every warp of the GPU instead of ending on one.
+//     subtree spreads over every warp of the GPU instead of ending on one.  A warp with
+//     some idle lanes and nothing to split inside takes published rows too.
 // The search step is search_step.cuh.  A lane's stack holds the sentinel entry at
 // `base` and its pending rows above it; giving away the bottom row turns that row's
 // slot into the new sentinel, so base moves up one slot.  Because pending rows are
@@ -144,6 +145,31 @@ __global__ void __launch_bounds__(BLOCK) batched_search_kernel(const BatchArgs a
     bool bad = false, qempty = false, stalled = false;
     uint32_t epoch = kEpoch, rounds = 0;
 
+    // An idle lane of rank `rank` < k takes ring row start + rank (bounded wait for its turn).
+    auto take_row = [&](uint32_t start, uint32_t k, bool mine, uint32_t rank) {
+        if (!mine || rank >= k) return;
+        const uint32_t idx = start + rank;
+        uint4* slot = a.ring + 2ull * (idx & (a.ring_cap - 1u));
+        uint32_t* turn = reinterpret_cast<uint32_t*>(slot + 1) + 2;
+        const uint32_t lap = idx >> a.ring_shift;
+        if (wait_turn(turn, 2u * lap + 1u, a.wait_limit)) {
+            const uint4 row = __ldcg(slot);
+            const uint4 meta = __ldcg(slot + 1);
+            st_release(turn, 2u * lap + 2u);
+            base = base0;
+            write_sentinel(base0);
+            s.avail = row.x;
+            s.nc = row.y;
+            s.l = row.z;
+            s.r = row.w;
+            s.sp = base;
+            item = meta.x;
+            weight = meta.y;
+        } else {
+            stalled = true;  // the row is lost: the launch reports a stall
+        }
+    };
+
     for (;;) {
         const bool me_idle = s.avail == 0 && s.sp == base;
         const uint32_t idle = __ballot_sync(kFull, me_idle);
@@ -235,31 +261,30 @@ __global__ void __launch_bounds__(BLOCK) batched_search_kernel(const BatchArgs a
                             stalled |= done == 2;
                             break;
                         }
-                        if (lane < k) {
-                            const uint32_t idx = start + lane;
-                            uint4* slot = a.ring + 2ull * (idx & (a.ring_cap - 1u));
-                            uint32_t* turn = reinterpret_cast<uint32_t*>(slot + 1) + 2;
-                            const uint32_t lap = idx >> a.ring_shift;
-                            if (wait_turn(turn, 2u * lap + 1u, a.wait_limit)) {
-                                const uint4 row = __ldcg(slot);
-                                const uint4 meta = __ldcg(slot + 1);
-                                st_release(turn, 2u * lap + 2u);
-                                base = base0;
-                                write_sentinel(base0);
-                                s.avail = row.x;
-                                s.nc = row.y;
-                                s.l = row.z;
-                                s.r = row.w;
-                                s.sp = base;
-                                item = meta.x;
-                                weight = meta.y;
-                            } else {
-                                stalled = true;  // the row is lost: the launch reports a stall
-                            }
-                        }
+                        take_row(start, k, true, lane);
                         __syncwarp();
                         if (lane == 0) atomicSub(hungry_warps, 1u);
                         rounds = 0;
+                    } else if (a.ring_cap) {
+                        // Some lanes idle and none to split from inside the warp: take rows
+                        // published in the ring, if there are any (no wait, not hungry).
+                        uint32_t k = 0, start = 0;
+                        if (lane == 0) {
+                            const unsigned long long ht =
+                                ld_relaxed64(reinterpret_cast<const unsigned long long*>(ring_head));
+                            const uint32_t h = (uint32_t)ht, t = (uint32_t)(ht >> 32);
+                            if (t != h) {
+                                const uint32_t want = min(t - h, (uint32_t)__popc(idle));
+                                if (atomicCAS(ring_head, h, h + want) == h) {
+                                    k = want;
+                                    start = h;
+                                }
+                            }
+                        }
+                        k = __shfl_sync(kFull, k, 0);
+                        start = __shfl_sync(kFull, start, 0);
+                        if (k) take_row(start, k, me_idle, __popc(idle & lt_mask));
+                        __syncwarp();
                     }
                 } else {
                     const uint32_t k = min(__popc(idle), __popc(donors));
@@ -299,10 +324,11 @@ __global__ void __launch_bounds__(BLOCK) batched_search_kernel(const BatchArgs a
         }
         // Publish rows for hungry warps: while the ring holds fewer than 32 rows per hungry
         // warp (and at most half its slots), lanes with pending rows give their bottom row.
-        // The tail only moves by a compare-and-swap against the snapshot the room was
-        // computed from, so the ring never holds more than half its slots and a producer
-        // never waits a lap.
-        if (a.ring_cap && qempty && ++rounds == kDonateEvery) {
+        // A warp whose lanes are all busy looks at the hungry count too: it need not have
+        // seen the item queue run dry itself (hungry warps exist only once it has).  The tail
+        // only moves by a compare-and-swap against the snapshot the room was computed from,
+        // so the ring never holds more than half its slots and a producer never waits a lap.
+        if (a.ring_cap && ++rounds == kDonateEvery) {
             rounds = 0;
             const uint32_t donors = __ballot_sync(kFull, s.sp != base);
             if (donors) {
