@@ -14,8 +14,7 @@
 //   - stealing across warps (when the launch has a steal ring): a warp with no work left
 //     registers as hungry and takes rows from a device ring; while hungry warps exist,
 //     busy warps publish the shallowest pending rows of their lanes into it, so a long
-//     subtree spreads over every warp of the GPU instead of ending on one.  A warp with
-//     some idle lanes and nothing to split inside takes published rows too.
+//     subtree spreads over every warp of the GPU instead of ending on one.
 // The search step is search_step.cuh.  A lane's stack holds the sentinel entry at
 // `base` and its pending rows above it; giving away the bottom row turns that row's
 // slot into the new sentinel, so base moves up one slot.  Because pending rows are
@@ -265,26 +264,6 @@ __global__ void __launch_bounds__(BLOCK) batched_search_kernel(const BatchArgs a
                         __syncwarp();
                         if (lane == 0) atomicSub(hungry_warps, 1u);
                         rounds = 0;
-                    } else if (a.ring_cap) {
-                        // Some lanes idle and none to split from inside the warp: take rows
-                        // published in the ring, if there are any (no wait, not hungry).
-                        uint32_t k = 0, start = 0;
-                        if (lane == 0) {
-                            const unsigned long long ht =
-                                ld_relaxed64(reinterpret_cast<const unsigned long long*>(ring_head));
-                            const uint32_t h = (uint32_t)ht, t = (uint32_t)(ht >> 32);
-                            if (t != h) {
-                                const uint32_t want = min(t - h, (uint32_t)__popc(idle));
-                                if (atomicCAS(ring_head, h, h + want) == h) {
-                                    k = want;
-                                    start = h;
-                                }
-                            }
-                        }
-                        k = __shfl_sync(kFull, k, 0);
-                        start = __shfl_sync(kFull, start, 0);
-                        if (k) take_row(start, k, me_idle, __popc(idle & lt_mask));
-                        __syncwarp();
                     }
                 } else {
                     const uint32_t k = min(__popc(idle), __popc(donors));
