@@ -114,7 +114,7 @@ __device__ __forceinline__ bool wait_turn(const uint32_t* turn, uint32_t want, u
     }
 }
 
-template <int BLOCK, bool LANES>
+template <int BLOCK, bool LANES, bool SPREAD>
 __global__ void __launch_bounds__(BLOCK) batched_search_kernel(const BatchArgs a) {
     extern __shared__ uint4 stack[];  // [stack_depth + 1][BLOCK]
     constexpr int kStride = BLOCK * 16;
@@ -169,6 +169,12 @@ __global__ void __launch_bounds__(BLOCK) batched_search_kernel(const BatchArgs a
         }
     };
 
+    // SPREAD (launches with fewer items than lanes): a refill claims only the warp's share of
+    // the items, so they spread over every warp before any splitting starts.  A separate
+    // instance: the same few instructions cost the large launches 2.5% (measured at N=21).
+    const uint32_t claim_cap =
+        SPREAD ? max(1u, (a.n_items + gridDim.x * (BLOCK / 32) - 1) / (gridDim.x * (BLOCK / 32))) : 0u;
+
     for (;;) {
         const bool me_idle = s.avail == 0 && s.sp == base;
         const uint32_t idle = __ballot_sync(kFull, me_idle);
@@ -187,13 +193,14 @@ __global__ void __launch_bounds__(BLOCK) batched_search_kernel(const BatchArgs a
                 piece_sols = piece_nodes = 0;
             }
             if (!qempty) {
-                const uint32_t k = __popc(idle);
+                const uint32_t k = SPREAD ? min((uint32_t)__popc(idle), claim_cap) : (uint32_t)__popc(idle);
                 uint32_t start = 0;
                 if (lane == 0) start = atomicAdd(a.ctl, k);
                 start = __shfl_sync(kFull, start, 0);
                 if (start + k >= a.n_items) qempty = true;
-                const uint32_t q = start + __popc(idle & lt_mask);
-                if (me_idle && q < a.n_items) {
+                const uint32_t ri = __popc(idle & lt_mask);
+                const uint32_t q = start + ri;
+                if (me_idle && (!SPREAD || ri < k) && q < a.n_items) {
                     const uint32_t it = a.order ? __ldg(a.order + q) : q;
                     const uint4 st = __ldg(a.items + it);
                     base = base0;
@@ -385,10 +392,13 @@ __global__ void __launch_bounds__(BLOCK) batched_search_kernel(const BatchArgs a
 
 template <int BLOCK, bool LANES>
 int launch_batched_t(const BatchArgs& a, int device, cudaStream_t stream, unsigned* launches) {
-    auto kern = batched_search_kernel<BLOCK, LANES>;
     const size_t smem = (size_t)(a.stack_depth + 1) * BLOCK * sizeof(uint4);
     if (smem > 227 * 1024) return NQB_E_RANGE;
+    auto kern = batched_search_kernel<BLOCK, LANES, false>;
+    auto spread = batched_search_kernel<BLOCK, LANES, true>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(spread, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return cuda_status(e);
     int sms = 0, per_sm = 0;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess)
@@ -400,7 +410,10 @@ int launch_batched_t(const BatchArgs& a, int device, cudaStream_t stream, unsign
     // One wave of blocks; with stealing, fewer items than lanes still fill the whole GPU.
     const uint64_t wave = (uint64_t)sms * per_sm;
     const unsigned grid = (unsigned)std::max<uint64_t>(1, a.ring_cap ? wave : std::min<uint64_t>(wave, need));
-    kern<<<grid, BLOCK, smem, stream>>>(a);
+    if (a.ring_cap && (uint64_t)a.n_items < (uint64_t)grid * BLOCK)
+        spread<<<grid, BLOCK, smem, stream>>>(a);
+    else
+        kern<<<grid, BLOCK, smem, stream>>>(a);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e);
     if (launches) (*launches)++;
