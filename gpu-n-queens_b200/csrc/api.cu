@@ -487,6 +487,10 @@ int nqb_batched_launch_ex(const nqb_state* d_items, uint64_t count, const uint32
                           uint64_t scratch_bytes, uint64_t* d_out, uint64_t* d_lane_stats, int block_size,
                           unsigned stack_depth, unsigned wait_limit, void* stream) {
     if (count > (1ull << 31)) return NQB_E_RANGE;
+    if (!d_out || !d_scratch || scratch_bytes < sizeof(uint32_t) || (count && !d_items)) return NQB_E_INVALID;
+    if (batched_ring_slots((size_t)scratch_bytes) && (reinterpret_cast<uintptr_t>(d_scratch) & 15) != 0)
+        return NQB_E_INVALID;  // the ring's words need 16-byte alignment
+    if (stack_depth > NQB_MAX_N) return NQB_E_INVALID;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return NQB_E_NODEVICE;
     return launch_batched(d_items, (uint32_t)count, d_order, nullptr, d_scratch, (size_t)scratch_bytes,

@@ -116,6 +116,17 @@ def test_new_entry_points_reject_bad_arguments_without_a_device(nqb):
     assert L.nqb_pool_for_target(8, 0, ctypes.byref(t)) == nqb.E_INVALID
     assert L.nqb_pool_for_target(40, 100, ctypes.byref(t)) == nqb.E_INVALID
     assert L.nqb_pool_for_target(8, 100, None) == nqb.E_INVALID
+    ex = L.nqb_batched_launch_ex
+    buf = ctypes.create_string_buffer(160)
+    base = ctypes.addressof(buf) + (-ctypes.addressof(buf)) % 16  # a 16-byte aligned host address
+    out = ctypes.c_uint64(0)
+    assert ex(None, 1 << 32, None, base, 64, ctypes.byref(out), None, 0, 0, 0, None) == nqb.E_RANGE
+    assert ex(None, 0, None, base, 64, None, None, 0, 0, 0, None) == nqb.E_INVALID          # no result words
+    assert ex(None, 0, None, None, 64, ctypes.byref(out), None, 0, 0, 0, None) == nqb.E_INVALID  # no scratch
+    assert ex(None, 0, None, base, 2, ctypes.byref(out), None, 0, 0, 0, None) == nqb.E_INVALID   # scratch < head
+    assert ex(None, 5, None, base, 64, ctypes.byref(out), None, 0, 0, 0, None) == nqb.E_INVALID  # items missing
+    assert ex(None, 0, None, base + 4, 128, ctypes.byref(out), None, 0, 0, 0, None) == nqb.E_INVALID  # ring unaligned
+    assert ex(None, 0, None, base, 64, ctypes.byref(out), None, 0, 32, 0, None) == nqb.E_INVALID  # stack depth > 31
 
 
 def test_c_program_links_and_runs(tmp_path):
