@@ -51,11 +51,11 @@ namespace {
 constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr uint32_t kNoItem = 0xFFFFFFFFu;
 #ifndef NQB_BATCHED_UNROLL
-#define NQB_BATCHED_UNROLL 32
+#define NQB_BATCHED_UNROLL 48
 #endif
 // Search steps between idle-lane checks.  Measured at N=19..21 (depth 7): 32 is 7% faster
-// than 16 (the per-round checks cost more than the idle lanes they save) and 64 is slower
-// again.
+// than 16 (the per-round checks cost more than the idle lanes they save), 48 another 0.75%,
+// and 64 is slower again.
 constexpr int kUnroll = NQB_BATCHED_UNROLL;
 constexpr uint32_t kEpoch = (1u << 27) / kUnroll;  // rounds between folds: 31 nodes x kUnroll x kEpoch < 2^32
 constexpr uint32_t kDonateEvery = 16;        // rounds between a busy warp's looks at the hungry count
