@@ -117,8 +117,9 @@ __device__ __forceinline__ uint32_t drop_leaves(uint32_t a, uint32_t nc, uint32_
     "not.b32 g, g;\n\t"                                                 \
     "and.b32 g, g, %1;\n\t"          /* G */                             \
     "neg.s32 x, g;\n\t"                                                 \
-    "and.b32 w, g, x;\n\t"                                              \
-    "setp.eq.u32 u, w, g;\n\t"       /* G has at most one column */      \
+    "not.b32 w, x;\n\t"                                                 \
+    "and.b32 w, w, g;\n\t"                                              \
+    "setp.eq.u32 u, w, 0;\n\t"       /* G has at most one column */      \
     "shr.s32 x, x, 31;\n\t"          /* all ones iff G != 0 */           \
     "mul.lo.u32 w, g, 7;\n\t"                                           \
     "shr.u32 w, w, 1;\n\t"           /* {g-1, g, g+1} */                 \
