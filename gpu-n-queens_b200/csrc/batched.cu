@@ -7,7 +7,9 @@
 // the grid is one wave of blocks over all SMs and each warp keeps its lanes busy:
 //   - refill: when lanes are idle and the queue still has items, the warp claims one
 //     item per idle lane with a single atomicAdd on the queue head; items are taken
-//     in the order of an optional permutation (e.g. largest predicted cost first);
+//     in the order of an optional permutation (e.g. largest predicted cost first).  With
+//     fewer items than the grid has lanes (the SPREAD instance) a warp claims only its
+//     share, so the items reach every warp before any splitting starts;
 //   - re-split inside the warp: once the queue is empty, a lane with pending rows hands
 //     its shallowest pending row (the largest piece of its remaining subtree) to an idle
 //     lane of the same warp, which searches it as a new piece of the same item;
