@@ -61,6 +61,9 @@ constexpr uint32_t kNoItem = 0xFFFFFFFFu;
 constexpr int kUnroll = NQB_BATCHED_UNROLL;
 constexpr uint32_t kEpoch = (1u << 27) / kUnroll;  // rounds between folds: 31 nodes x kUnroll x kEpoch < 2^32
 constexpr uint32_t kDonateEvery = 16;        // rounds between a busy warp's looks at the hungry count
+// The spread instance (launches with fewer items than lanes) looks 4x less often: on coarse
+// pools that measured 2-6% faster (N=17..20, depth 3-4; smaller pieces cost ring traffic).
+constexpr uint32_t kDonateEverySpread = 4 * kDonateEvery;
 
 // Error flags written to out[3].
 constexpr unsigned long long kErrStack = 1ull;  // an item needed a deeper stack than provided
@@ -316,7 +319,7 @@ __global__ void __launch_bounds__(BLOCK) batched_search_kernel(const BatchArgs a
         // seen the item queue run dry itself (hungry warps exist only once it has).  The tail
         // only moves by a compare-and-swap against the snapshot the room was computed from,
         // so the ring never holds more than half its slots and a producer never waits a lap.
-        if (a.ring_cap && ++rounds == kDonateEvery) {
+        if (a.ring_cap && ++rounds == (SPREAD ? kDonateEverySpread : kDonateEvery)) {
             rounds = 0;
             const uint32_t donors = __ballot_sync(kFull, s.sp != base);
             if (donors) {
