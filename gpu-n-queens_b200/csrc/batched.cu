@@ -61,9 +61,11 @@ constexpr uint32_t kNoItem = 0xFFFFFFFFu;
 constexpr int kUnroll = NQB_BATCHED_UNROLL;
 constexpr uint32_t kEpoch = (1u << 27) / kUnroll;  // rounds between folds: 31 nodes x kUnroll x kEpoch < 2^32
 constexpr uint32_t kDonateEvery = 16;        // rounds between a busy warp's looks at the hungry count
-// The spread instance (launches with fewer items than lanes) looks 4x less often: on coarse
-// pools that measured 2-6% faster (N=17..20, depth 3-4; smaller pieces cost ring traffic).
-constexpr uint32_t kDonateEverySpread = 4 * kDonateEvery;
+// The spread instance (launches with fewer items than lanes) looks 8x less often.  Measured on
+// coarse pools against every 16 and 64 rounds: N=19 d=4 215 / 205 / 196 ms, N=20 d=4 1400 /
+// 1385 / 1373 ms, the 65,536 uneven boards 1836 ms at 64 and 1824 ms at 128; only the smallest
+// launch (N=17 d=3, 9 ms) is faster at 64, by 0.5 ms.  256 is no better than 128.
+constexpr uint32_t kDonateEverySpread = 8 * kDonateEvery;
 
 // Error flags written to out[3].
 constexpr unsigned long long kErrStack = 1ull;  // an item needed a deeper stack than provided
