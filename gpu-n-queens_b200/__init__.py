@@ -120,6 +120,7 @@ def lib():
                                                       u64p, ctypes.POINTER(Stats)]),
             "nqb_device_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
             "nqb_trim_device_memory": (ctypes.c_int, [ctypes.c_int]),
+            "nqb_debug_fail_allocation": (ctypes.c_longlong, [ctypes.c_longlong]),
             "nqb_measure_int32_peak": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                                       ctypes.POINTER(ctypes.c_double)]),
         }
@@ -327,6 +328,13 @@ def measure_int32_peak(device=0):
 def trim_device_memory(device=0):
     """Returns the library's cached device memory on `device` to the driver."""
     _check(lib().nqb_trim_device_memory(device), "nqb_trim_device_memory")
+
+
+def debug_fail_allocation(after):
+    """Test hook (nqb_debug_fail_allocation): the library's next `after` allocations succeed and
+    the one after them fails as out of memory; a negative value turns the hook off.  Returns the
+    countdown it replaces (-1: the hook was off or has fired)."""
+    return int(lib().nqb_debug_fail_allocation(after))
 
 
 def device_count():

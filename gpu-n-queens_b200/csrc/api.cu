@@ -6,6 +6,7 @@
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <thread>
 #include <vector>
 
@@ -54,18 +55,27 @@ class Scope {
         if (stream) cudaStreamDestroy(stream);
         cudaSetDevice(prev_);
     }
+    // The slot is added before the buffer or event is made: a push_back that throws then
+    // leaves nothing behind.
     template <class T>
     int alloc(T** p, size_t bytes) {
-        void* v = nullptr;
-        const int s = dev_alloc_bytes(&v, bytes, stream);
-        if (s != NQB_OK) return s;
-        bufs_.push_back(v);
-        *p = static_cast<T*>(v);
+        bufs_.push_back(nullptr);
+        const int s = dev_alloc_bytes(&bufs_.back(), bytes, stream);
+        if (s != NQB_OK) {
+            bufs_.pop_back();
+            return s;
+        }
+        *p = static_cast<T*>(bufs_.back());
         return NQB_OK;
     }
     int event(cudaEvent_t* e) {
-        const int s = cuda_status(cudaEventCreate(e));
-        if (s == NQB_OK) events_.push_back(*e);
+        events_.push_back(nullptr);
+        const int s = cuda_status(cudaEventCreate(&events_.back()));
+        if (s != NQB_OK) {
+            events_.pop_back();
+            return s;
+        }
+        *e = events_.back();
         return s;
     }
     Scope(const Scope&) = delete;
@@ -184,6 +194,7 @@ int solve_host_states(Scope& sc, const nqb_state* states, uint64_t count, const 
 
 void* aligned_host_alloc(size_t bytes) {
     void* p = nullptr;
+    if (alloc_fault()) return nullptr;
     if (posix_memalign(&p, 64, bytes ? bytes : 64)) return nullptr;
     return p;
 }
@@ -251,34 +262,31 @@ int nqb_device_check(int device) {
 
 void nqb_free(void* p) { std::free(p); }
 
-int nqb_generate_pool_into(unsigned n, unsigned depth, nqb_state* buf, uint64_t capacity, uint64_t* count) {
+int nqb_generate_pool_into(unsigned n, unsigned depth, nqb_state* buf, uint64_t capacity, uint64_t* count) try {
     if (!count) return NQB_E_INVALID;
     return generate_pool(n, depth, buf, buf ? capacity : 0, count, nullptr);
-}
+} NQB_ABI_CATCH
 
-int nqb_pool_weighted_size(unsigned n, unsigned depth, uint64_t* weighted) {
+int nqb_pool_weighted_size(unsigned n, unsigned depth, uint64_t* weighted) try {
     if (!weighted) return NQB_E_INVALID;
     uint64_t c = 0;
     return generate_pool(n, depth, nullptr, 0, &c, weighted);
-}
+} NQB_ABI_CATCH
 
-int nqb_generate_pool(unsigned n, unsigned depth, nqb_state** states, uint64_t* count) {
+int nqb_generate_pool(unsigned n, unsigned depth, nqb_state** states, uint64_t* count) try {
     if (!states || !count) return NQB_E_INVALID;
     *states = nullptr;
     uint64_t c = 0;
     NQB_TRY(generate_pool(n, depth, nullptr, 0, &c, nullptr));
-    nqb_state* p = static_cast<nqb_state*>(aligned_host_alloc(c * sizeof(nqb_state)));
+    std::unique_ptr<nqb_state, void (*)(void*)> p(static_cast<nqb_state*>(aligned_host_alloc(c * sizeof(nqb_state))),
+                                                  std::free);
     if (!p) return NQB_E_NOMEM;
-    const int s = generate_pool(n, depth, p, c, count, nullptr);
-    if (s != NQB_OK) {
-        std::free(p);
-        return s;
-    }
-    *states = p;
+    NQB_TRY(generate_pool(n, depth, p.get(), c, count, nullptr));
+    *states = p.release();
     return NQB_OK;
-}
+} NQB_ABI_CATCH
 
-int nqb_count_ex(unsigned n, unsigned depth, const nqb_opts* opts, uint64_t* count, nqb_stats* stats) {
+int nqb_count_ex(unsigned n, unsigned depth, const nqb_opts* opts, uint64_t* count, nqb_stats* stats) try {
     const double t0 = now_ms();
     if (!count || n < NQB_MIN_N || n > NQB_MAX_N || depth < 1 || depth >= n) return NQB_E_INVALID;
     nqb_opts o = resolve(opts);
@@ -299,11 +307,10 @@ int nqb_count_ex(unsigned n, unsigned depth, const nqb_opts* opts, uint64_t* cou
         uint64_t cnt = 0;
         const double tg = now_ms();
         NQB_TRY(nqb_generate_pool(n, depth, &pool, &cnt));
+        std::unique_ptr<nqb_state, void (*)(void*)> own(pool, std::free);
         gen_ms = now_ms() - tg;
-        const int s = solve_host_states(sc, pool, cnt, o, totals, nullptr, stats, nullptr,
-                                        n - depth - 1 > 0 ? n - depth - 1 : 1);
-        std::free(pool);
-        NQB_TRY(s);
+        NQB_TRY(solve_host_states(sc, pool, cnt, o, totals, nullptr, stats, nullptr,
+                                  n - depth - 1 > 0 ? n - depth - 1 : 1));
     } else {  // build the pool on the GPU: nothing crosses PCIe but the result
         cudaEvent_t g0, g1;
         NQB_TRY(sc.event(&g0));
@@ -328,12 +335,12 @@ int nqb_count_ex(unsigned n, unsigned depth, const nqb_opts* opts, uint64_t* cou
         stats->wall_ms = now_ms() - t0;
     }
     return NQB_OK;
-}
+} NQB_ABI_CATCH
 
 int nqb_count(unsigned n, unsigned depth, uint64_t* count) { return nqb_count_ex(n, depth, nullptr, count, nullptr); }
 
 int nqb_solve_states(const nqb_state* states, uint64_t count, const nqb_opts* opts, uint64_t* total,
-                     nqb_stats* stats) {
+                     nqb_stats* stats) try {
     const double t0 = now_ms();
     if (!total || (count && !states)) return NQB_E_INVALID;
     if (stats) std::memset(stats, 0, sizeof(*stats));
@@ -347,10 +354,10 @@ int nqb_solve_states(const nqb_state* states, uint64_t count, const nqb_opts* op
     *total = totals[0];
     if (stats) stats->wall_ms = now_ms() - t0;
     return NQB_OK;
-}
+} NQB_ABI_CATCH
 
 int nqb_solve_states_multi(const nqb_state* states, uint64_t count, const int* devices, unsigned ndev,
-                           const nqb_opts* opts, uint64_t* total, nqb_stats* stats) {
+                           const nqb_opts* opts, uint64_t* total, nqb_stats* stats) try {
     const double t0 = now_ms();
     if (!total || (count && !states) || !devices || ndev == 0) return NQB_E_INVALID;
     if (stats) std::memset(stats, 0, sizeof(*stats));
@@ -391,10 +398,10 @@ int nqb_solve_states_multi(const nqb_state* states, uint64_t count, const int* d
         stats->wall_ms = now_ms() - t0;
     }
     return NQB_OK;
-}
+} NQB_ABI_CATCH
 
 int nqb_solve_batch(const nqb_state* boards, uint64_t count, const nqb_opts* opts, uint64_t* out,
-                    nqb_stats* stats) {
+                    nqb_stats* stats) try {
     const double t0 = now_ms();
     if (!out || (count && !boards)) return NQB_E_INVALID;
     if (stats) std::memset(stats, 0, sizeof(*stats));
@@ -406,10 +413,10 @@ int nqb_solve_batch(const nqb_state* boards, uint64_t count, const nqb_opts* opt
     NQB_TRY(solve_host_states(sc, boards, count, o, totals, out, stats));
     if (stats) stats->wall_ms = now_ms() - t0;
     return NQB_OK;
-}
+} NQB_ABI_CATCH
 
 int nqb_record_nodes(const nqb_state* states, uint64_t count, const nqb_opts* opts, uint64_t* nodes,
-                     uint64_t* counts) {
+                     uint64_t* counts) try {
     if (!nodes || !counts || (count && !states)) return NQB_E_INVALID;
     if (count == 0) return NQB_OK;
     nqb_opts o = resolve(opts);
@@ -419,7 +426,7 @@ int nqb_record_nodes(const nqb_state* states, uint64_t count, const nqb_opts* op
     NQB_TRY(sc.status);
     unsigned long long totals[4] = {0, 0, 0, 0};
     return solve_host_states(sc, states, count, o, totals, counts, nullptr, nodes);
-}
+} NQB_ABI_CATCH
 
 size_t nqb_ref_state_size(unsigned n) {
     if (n < 1 || n > NQB_MAX_N) return 0;
@@ -452,7 +459,7 @@ int nqb_states_from_ref(unsigned n, const void* ref_states, uint64_t count, int 
 }
 
 int nqb_solve_ref_states(unsigned n, const void* ref_states, uint64_t count, unsigned locked_row,
-                         const nqb_opts* opts, uint64_t* total) {
+                         const nqb_opts* opts, uint64_t* total) try {
     if (!total || n < NQB_MIN_N || n > NQB_MAX_N || locked_row < 1 || locked_row >= n) return NQB_E_INVALID;
     if (count && !ref_states) return NQB_E_INVALID;
     *total = 0;
@@ -465,27 +472,27 @@ int nqb_solve_ref_states(unsigned n, const void* ref_states, uint64_t count, uns
     if (s == NQB_OK) s = nqb_solve_states(st, count, opts, total, nullptr);
     std::free(st);
     return s;
-}
+} NQB_ABI_CATCH
 
 int nqb_plain_launch(const nqb_state* d_states, uint64_t count, uint64_t* d_out, int block_size,
-                     int count_unit_nodes, unsigned stack_depth, void* stream) {
+                     int count_unit_nodes, unsigned stack_depth, void* stream) try {
     return launch_plain(d_states, count, reinterpret_cast<unsigned long long*>(d_out), nullptr, block_size,
                         count_unit_nodes != 0, stack_depth, static_cast<cudaStream_t>(stream), nullptr);
-}
+} NQB_ABI_CATCH
 
 int nqb_batched_launch(const nqb_state* d_items, uint64_t count, const uint32_t* d_order, uint32_t* d_head,
-                       uint64_t* d_out, int block_size, unsigned stack_depth, void* stream) {
+                       uint64_t* d_out, int block_size, unsigned stack_depth, void* stream) try {
     if (count > (1ull << 31)) return NQB_E_RANGE;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return NQB_E_NODEVICE;
     return launch_batched(d_items, (uint32_t)count, d_order, nullptr, d_head, sizeof(uint32_t),
                           reinterpret_cast<unsigned long long*>(d_out), nullptr, nullptr, block_size, stack_depth, dev,
                           static_cast<cudaStream_t>(stream), nullptr);
-}
+} NQB_ABI_CATCH
 
 int nqb_batched_launch_ex(const nqb_state* d_items, uint64_t count, const uint32_t* d_order, void* d_scratch,
                           uint64_t scratch_bytes, uint64_t* d_out, uint64_t* d_lane_stats, int block_size,
-                          unsigned stack_depth, unsigned wait_limit, void* stream) {
+                          unsigned stack_depth, unsigned wait_limit, void* stream) try {
     if (count > (1ull << 31)) return NQB_E_RANGE;
     if (!d_out || !d_scratch || scratch_bytes < sizeof(uint32_t) || (count && !d_items)) return NQB_E_INVALID;
     if (batched_ring_slots((size_t)scratch_bytes) && (reinterpret_cast<uintptr_t>(d_scratch) & 15) != 0)
@@ -497,15 +504,15 @@ int nqb_batched_launch_ex(const nqb_state* d_items, uint64_t count, const uint32
                           reinterpret_cast<unsigned long long*>(d_out), nullptr, nullptr, block_size, stack_depth, dev,
                           static_cast<cudaStream_t>(stream), nullptr,
                           reinterpret_cast<unsigned long long*>(d_lane_stats), wait_limit);
-}
+} NQB_ABI_CATCH
 
-int nqb_generate_pool_device(unsigned n, unsigned depth, nqb_state** d_states, uint64_t* count, void* stream) {
+int nqb_generate_pool_device(unsigned n, unsigned depth, nqb_state** d_states, uint64_t* count, void* stream) try {
     if (!d_states || !count) return NQB_E_INVALID;
     return generate_pool_device(n, depth, static_cast<cudaStream_t>(stream), d_states, count);
-}
+} NQB_ABI_CATCH
 
 int nqb_generate_pool_device_into(unsigned n, unsigned depth, nqb_state* d_buf, uint64_t capacity, uint64_t* count,
-                                  void* stream) {
+                                  void* stream) try {
     if (!count || (capacity && !d_buf)) return NQB_E_INVALID;
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
     nqb_state* d_pool = nullptr;
@@ -515,7 +522,7 @@ int nqb_generate_pool_device_into(unsigned n, unsigned depth, nqb_state* d_buf, 
     else if (*count) s = cuda_status(cudaMemcpyAsync(d_buf, d_pool, *count * sizeof(nqb_state), cudaMemcpyDeviceToDevice, st));
     dev_free(d_pool, st);
     return s;
-}
+} NQB_ABI_CATCH
 
 void nqb_free_device(void* p, void* stream) {
     dev_free(p, static_cast<cudaStream_t>(stream));

@@ -521,7 +521,7 @@ int static_scratch_address(int dev, uint32_t** out) {
 }  // namespace
 
 extern "C" int nqb_batched_launch_static(const nqb_state* d_items, uint64_t count, const uint32_t* d_order,
-                                         uint64_t* d_out, int block_size, unsigned stack_depth, void* stream) {
+                                         uint64_t* d_out, int block_size, unsigned stack_depth, void* stream) try {
     if (count > NQB_STATIC_MAX_ITEMS) return NQB_E_RANGE;
     if (!d_out || (count && !d_items)) return NQB_E_INVALID;
     int dev = 0;
@@ -537,4 +537,4 @@ extern "C" int nqb_batched_launch_static(const nqb_state* d_items, uint64_t coun
     return nqb::launch_batched(d_items, (uint32_t)count, d_order, nullptr, head, sizeof(uint32_t),
                                reinterpret_cast<unsigned long long*>(d_out), nullptr, nullptr, block_size,
                                stack_depth, dev, st, nullptr);
-}
+} NQB_ABI_CATCH

@@ -4,6 +4,7 @@
 // returns what is cached.
 #include <cuda.h>
 
+#include <atomic>
 #include <mutex>
 
 #include "nqb_internal.h"
@@ -72,8 +73,20 @@ int device_pool(int dev, cudaMemPool_t* out) {
 
 }  // namespace
 
+// Allocations left before the one that fails; -1: the hook is off (nqb_debug_fail_allocation).
+std::atomic<long long> g_fail_countdown{-1};
+
+bool alloc_fault() {
+    long long v = g_fail_countdown.load(std::memory_order_relaxed);
+    while (v >= 0) {  // count this allocation down; the one that takes the countdown to -1 fails
+        if (g_fail_countdown.compare_exchange_weak(v, v - 1, std::memory_order_relaxed)) return v == 0;
+    }
+    return false;
+}
+
 int dev_alloc_bytes(void** p, size_t bytes, cudaStream_t s) {
     *p = nullptr;
+    if (alloc_fault()) return NQB_E_NOMEM;
     int dev = 0;
     NQB_TRY(cuda_status(cudaGetDevice(&dev)));
     cudaMemPool_t pool = nullptr;
@@ -86,6 +99,10 @@ void dev_free(void* p, cudaStream_t s) {
 }
 
 }  // namespace nqb
+
+extern "C" long long nqb_debug_fail_allocation(long long after) {
+    return nqb::g_fail_countdown.exchange(after < 0 ? -1 : after);
+}
 
 extern "C" int nqb_trim_device_memory(int device) {
     if (device < 0 || device >= nqb::kMaxDevices) return NQB_E_NODEVICE;

@@ -548,9 +548,10 @@ struct Work {
     int init(uint32_t rows) {
         cap = rows;
         const size_t r = rows;
+        owned.reserve(16);  // may throw, but before anything is allocated; push_back then does not
         auto get = [&](auto** p, size_t bytes) {
             void* v = nullptr;
-            const int s = cuda_status(cudaMalloc(&v, bytes ? bytes : 16));
+            const int s = cuda_malloc(&v, bytes);
             if (s == NQB_OK) {
                 owned.push_back(v);
                 *p = static_cast<std::remove_pointer_t<decltype(p)>>(v);
@@ -691,7 +692,7 @@ struct CallScope {  // current device for the call, restored afterwards; one str
 template <class T>
 struct DevBuf {
     T* p = nullptr;
-    int alloc(size_t n) { return cuda_status(cudaMalloc(&p, (n ? n : 1) * sizeof(T))); }
+    int alloc(size_t n) { return cuda_malloc(&p, (n ? n : 1) * sizeof(T)); }
     ~DevBuf() {
         if (p) cudaFree(p);
     }
@@ -706,23 +707,23 @@ int refresh_half(nqb_model* m, cudaStream_t s) {
 
 extern "C" {
 
-int nqb_model_create(int device, uint64_t seed, nqb_model** out) {
+int nqb_model_create(int device, uint64_t seed, nqb_model** out) try {
     if (!out) return NQB_E_INVALID;
     *out = nullptr;
     int st = nqb_device_check(device);
     if (st) return st;
     CallScope cs(device);
     if (cs.status) return cs.status;
+    std::vector<float> p;  // before the model object: nothing to release if this throws
+    init_params(p, seed);
     nqb_model* m = new nqb_model();
     m->device = device;
-    std::vector<float> p;
-    init_params(p, seed);
-    st = cuda_status(cudaMalloc(&m->params, kParams * sizeof(float)));
-    if (!st) st = cuda_status(cudaMalloc(&m->grad, kParams * sizeof(float)));
-    if (!st) st = cuda_status(cudaMalloc(&m->m, kParams * sizeof(float)));
-    if (!st) st = cuda_status(cudaMalloc(&m->v, kParams * sizeof(float)));
-    if (!st) st = cuda_status(cudaMalloc(&m->w1h, kW1Size * sizeof(__half)));
-    if (!st) st = cuda_status(cudaMalloc(&m->w2h, kH * kH * sizeof(__half)));
+    st = cuda_malloc(&m->params, kParams * sizeof(float));
+    if (!st) st = cuda_malloc(&m->grad, kParams * sizeof(float));
+    if (!st) st = cuda_malloc(&m->m, kParams * sizeof(float));
+    if (!st) st = cuda_malloc(&m->v, kParams * sizeof(float));
+    if (!st) st = cuda_malloc(&m->w1h, kW1Size * sizeof(__half));
+    if (!st) st = cuda_malloc(&m->w2h, kH * kH * sizeof(__half));
     if (!st) st = cuda_status(cudaMemcpyAsync(m->params, p.data(), kParams * sizeof(float), cudaMemcpyHostToDevice, cs.s));
     if (!st) st = cuda_status(cudaMemsetAsync(m->m, 0, kParams * sizeof(float), cs.s));
     if (!st) st = cuda_status(cudaMemsetAsync(m->v, 0, kParams * sizeof(float), cs.s));
@@ -734,7 +735,7 @@ int nqb_model_create(int device, uint64_t seed, nqb_model** out) {
     }
     *out = m;
     return NQB_OK;
-}
+} NQB_ABI_CATCH
 
 void nqb_model_destroy(nqb_model* m) {
     if (!m) return;
@@ -773,7 +774,7 @@ int nqb_model_set_params(nqb_model* m, const float* in) {
     return st;
 }
 
-int nqb_model_features(const nqb_state* states, uint64_t count, float* out) {
+int nqb_model_features(const nqb_state* states, uint64_t count, float* out) try {
     if (count && (!states || !out)) return NQB_E_INVALID;
     for (uint64_t i = 0; i < count; ++i) {
         uint4 st;
@@ -781,14 +782,14 @@ int nqb_model_features(const nqb_state* states, uint64_t count, float* out) {
         for (int j = 0; j < kIn; ++j) out[i * kIn + j] = feature(st, j);
     }
     return NQB_OK;
-}
+} NQB_ABI_CATCH
 
-int nqb_model_predict(const nqb_model* m, const nqb_state* states, uint64_t count, float* out) {
+int nqb_model_predict(const nqb_model* m, const nqb_state* states, uint64_t count, float* out) try {
     return nqb_model_predict_ex(m, states, count, out, 0);
-}
+} NQB_ABI_CATCH
 
 int nqb_model_predict_ex(const nqb_model* m, const nqb_state* states, uint64_t count, float* out,
-                         uint32_t wait_limit) {
+                         uint32_t wait_limit) try {
     if (!m || (count && (!states || !out))) return NQB_E_INVALID;
     if (count == 0) return NQB_OK;
     if (count > 0xFFFFFFFFull) return NQB_E_RANGE;
@@ -803,10 +804,10 @@ int nqb_model_predict_ex(const nqb_model* m, const nqb_state* states, uint64_t c
     if (!st) st = cuda_status(cudaMemcpyAsync(out, d_out.p, count * sizeof(float), cudaMemcpyDeviceToHost, cs.s));
     if (!st) st = cuda_status(cudaStreamSynchronize(cs.s));
     return st;
-}
+} NQB_ABI_CATCH
 
 int nqb_model_loss_grad(nqb_model* m, const nqb_state* states, const float* targets, uint64_t count, float* loss,
-                        float* grad) {
+                        float* grad) try {
     if (!m || !states || !targets || !loss || !grad || count == 0) return NQB_E_INVALID;
     if (count > (1u << 20)) return NQB_E_RANGE;
     CallScope cs(m->device);
@@ -828,10 +829,10 @@ int nqb_model_loss_grad(nqb_model* m, const nqb_state* states, const float* targ
     if (!st) st = w.check(cs.s);
     *loss = l / (float)count;
     return st;
-}
+} NQB_ABI_CATCH
 
 int nqb_model_train(nqb_model* m, const nqb_state* states, const float* targets, uint64_t count,
-                    const nqb_train_opts* opts, float* epoch_loss) {
+                    const nqb_train_opts* opts, float* epoch_loss) try {
     if (!m || !states || !targets || count == 0) return NQB_E_INVALID;
     if (count > 0xFFFFFFFFull) return NQB_E_RANGE;
     nqb_train_opts o;
@@ -892,7 +893,7 @@ int nqb_model_train(nqb_model* m, const nqb_state* states, const float* targets,
         if (epoch_loss) epoch_loss[ep] = l / (float)count;
     }
     return cuda_status(cudaStreamSynchronize(cs.s));
-}
+} NQB_ABI_CATCH
 
 }  // extern "C"
 

@@ -14,6 +14,17 @@
         if (s_ != NQB_OK) return s_; \
     } while (0)
 
+// Handler of the C ABI entry points, each written as a function-try-block
+// (`int nqb_f(...) try { ... } NQB_ABI_CATCH`), so that no C++ exception crosses the C ABI.
+// The library throws none of its own.  The standard library's containers, `new` and
+// std::thread throw when host memory or threads run out (std::bad_alloc, std::length_error,
+// std::system_error); the entry point then returns NQB_E_NOMEM.  The body's objects are
+// destroyed on the way out, so the device buffers, streams and events they own are released.
+#define NQB_ABI_CATCH       \
+    catch (...) {           \
+        return NQB_E_NOMEM; \
+    }
+
 namespace nqb {
 
 inline uint32_t board_mask(unsigned n) { return n >= 32 ? 0xFFFFFFFFu : ((1u << n) - 1u); }
@@ -117,6 +128,32 @@ int dev_alloc(T** p, size_t bytes, cudaStream_t s) {
 void dev_free(void* p, cudaStream_t s);
 
 int cuda_status(cudaError_t e);
+
+// The allocation-failure test hook (nqb_debug_fail_allocation, devmem.cu): true when the
+// allocation being made now is the one chosen to fail.  Every allocation of the library's own
+// code asks it first: device buffers (dev_alloc_bytes, cuda_malloc), pinned host buffers
+// (cuda_malloc_host) and host buffers (the pool and state-file arrays).
+bool alloc_fault();
+
+// cudaMalloc and cudaMallocHost behind the test hook; *p is nullptr unless NQB_OK.
+template <class T>
+int cuda_malloc(T** p, size_t bytes) {
+    *p = nullptr;
+    if (alloc_fault()) return NQB_E_NOMEM;
+    void* v = nullptr;
+    const int s = cuda_status(cudaMalloc(&v, bytes ? bytes : 16));
+    if (s == NQB_OK) *p = static_cast<T*>(v);
+    return s;
+}
+template <class T>
+int cuda_malloc_host(T** p, size_t bytes) {
+    *p = nullptr;
+    if (alloc_fault()) return NQB_E_NOMEM;
+    void* v = nullptr;
+    const int s = cuda_status(cudaMallocHost(&v, bytes ? bytes : 16));
+    if (s == NQB_OK) *p = static_cast<T*>(v);
+    return s;
+}
 
 // Unique id of the calling thread's current CUDA context, 0 when none (devmem.cu).
 unsigned long long current_context_id();

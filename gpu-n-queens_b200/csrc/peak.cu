@@ -73,7 +73,7 @@ int time_kind(int sms, uint32_t iters, uint32_t* d_out, cudaStream_t s, double* 
 }  // namespace
 }  // namespace nqb
 
-extern "C" int nqb_measure_int32_peak(int device, double* best, double* per_kind) {
+extern "C" int nqb_measure_int32_peak(int device, double* best, double* per_kind) try {
     using namespace nqb;
     if (!best) return NQB_E_INVALID;
     *best = 0;
@@ -105,4 +105,4 @@ extern "C" int nqb_measure_int32_peak(int device, double* best, double* per_kind
         if (r[k] > *best) *best = r[k];
     }
     return NQB_OK;
-}
+} NQB_ABI_CATCH

@@ -189,7 +189,7 @@ void nqb_batch_plan_destroy(nqb_batch_plan* p) {
 }
 
 int nqb_batch_plan_create(const nqb_state* boards, uint64_t count, const nqb_opts* opts, int autotune,
-                          nqb_batch_plan** out) {
+                          nqb_batch_plan** out) try {
     if (!out || !boards || count == 0) return NQB_E_INVALID;
     *out = nullptr;
     if (count > (1ull << 31)) return NQB_E_RANGE;
@@ -198,6 +198,14 @@ int nqb_batch_plan_create(const nqb_state* boards, uint64_t count, const nqb_opt
     if (opts) o = *opts;
     for (uint64_t i = 0; i < count; ++i)
         if (!nqb::state_valid(boards[i])) return NQB_E_INVALID;
+    std::vector<int> blocks, factors;  // built before anything that needs releasing
+    if (autotune) {
+        blocks = {64, 128, 256};
+        factors = (o.model || o.sched_cost) ? std::vector<int>{1, 4, 16} : std::vector<int>{o.split_factor};
+    } else {
+        blocks = {o.block_size ? o.block_size : 128};
+        factors = {o.split_factor};
+    }
     int st = nqb_device_check(o.device);
     if (st) return st;
     nqb_batch_plan* p = new nqb_batch_plan();
@@ -211,25 +219,17 @@ int nqb_batch_plan_create(const nqb_state* boards, uint64_t count, const nqb_opt
     };
     if ((st = cuda_status(cudaSetDevice(p->device)))) return fail(st);
     if ((st = cuda_status(cudaStreamCreateWithFlags(&p->s, cudaStreamNonBlocking)))) return fail(st);
-    if ((st = cuda_status(cudaMalloc(&p->d_boards, count * sizeof(nqb_state))))) return fail(st);
-    if ((st = cuda_status(cudaMalloc(&p->d_per, count * sizeof(unsigned long long))))) return fail(st);
-    if ((st = cuda_status(cudaMalloc(&p->d_out, 8 * sizeof(unsigned long long) + nqb::kBatchedScratchBytes))))
+    if ((st = nqb::cuda_malloc(&p->d_boards, count * sizeof(nqb_state)))) return fail(st);
+    if ((st = nqb::cuda_malloc(&p->d_per, count * sizeof(unsigned long long)))) return fail(st);
+    if ((st = nqb::cuda_malloc(&p->d_out, 8 * sizeof(unsigned long long) + nqb::kBatchedScratchBytes)))
         return fail(st);
-    if ((st = cuda_status(cudaMalloc(&p->d_split, sizeof(unsigned long long))))) return fail(st);
-    if ((st = cuda_status(cudaMallocHost(&p->h_per, count * sizeof(unsigned long long))))) return fail(st);
-    if ((st = cuda_status(cudaMallocHost(&p->h_out, 4 * sizeof(unsigned long long))))) return fail(st);
+    if ((st = nqb::cuda_malloc(&p->d_split, sizeof(unsigned long long)))) return fail(st);
+    if ((st = nqb::cuda_malloc_host(&p->h_per, count * sizeof(unsigned long long)))) return fail(st);
+    if ((st = nqb::cuda_malloc_host(&p->h_out, 4 * sizeof(unsigned long long)))) return fail(st);
     if ((st = cuda_status(cudaMemcpyAsync(p->d_boards, boards, count * sizeof(nqb_state), cudaMemcpyHostToDevice,
                                           p->s))))
         return fail(st);
 
-    std::vector<int> blocks, factors;
-    if (autotune) {
-        blocks = {64, 128, 256};
-        factors = (o.model || o.sched_cost) ? std::vector<int>{1, 4, 16} : std::vector<int>{o.split_factor};
-    } else {
-        blocks = {o.block_size ? o.block_size : 128};
-        factors = {o.split_factor};
-    }
     int best_block = blocks[0], best_factor = factors[0];
     if (blocks.size() * factors.size() > 1 &&
         (st = tune_on_sample(p, o, blocks, factors, &best_block, &best_factor)))
@@ -240,7 +240,7 @@ int nqb_batch_plan_create(const nqb_state* boards, uint64_t count, const nqb_opt
     *out = p;
     cudaSetDevice(p->prev_device);
     return NQB_OK;
-}
+} NQB_ABI_CATCH
 
 int nqb_batch_plan_run(nqb_batch_plan* p, uint64_t* out, nqb_stats* stats) {
     if (!p || !out) return NQB_E_INVALID;

@@ -199,7 +199,7 @@ struct SplitMix64 {
 }  // namespace
 
 extern "C" int nqb_sample_boards(uint64_t seed, uint64_t count, unsigned n_min, unsigned n_max, unsigned d_min,
-                                 unsigned d_max, nqb_state* out) {
+                                 unsigned d_max, nqb_state* out) try {
     if ((count && !out) || n_min < NQB_MIN_N || n_max > NQB_MAX_N || n_min > n_max || d_min < 1 || d_min > d_max ||
         d_max >= n_min)
         return NQB_E_INVALID;
@@ -233,4 +233,4 @@ extern "C" int nqb_sample_boards(uint64_t seed, uint64_t count, unsigned n_min, 
         s.flags = 0;
     }
     return NQB_OK;
-}
+} NQB_ABI_CATCH

@@ -31,7 +31,9 @@ struct Out {
     FILE* f;
     std::vector<uint8_t> buf;
     bool bad = false;
-    explicit Out(FILE* fp) : f(fp) { buf.reserve(1 << 20); }
+    // The buffer is sized once (it may throw then) and a flush empties it before it
+    // would grow, so writing never allocates.
+    explicit Out(FILE* fp) : f(fp) { buf.reserve((1 << 20) + 64); }
     void flush() {
         if (!buf.empty() && std::fwrite(buf.data(), 1, buf.size(), f) != buf.size()) bad = true;
         buf.clear();
@@ -78,12 +80,13 @@ using namespace nqb;
 
 extern "C" {
 
-int nqb_generate_pool_placements(unsigned n, unsigned depth, nqb_placement** placements, uint64_t* count) {
+int nqb_generate_pool_placements(unsigned n, unsigned depth, nqb_placement** placements, uint64_t* count) try {
     if (!placements || !count) return NQB_E_INVALID;
     *placements = nullptr;
     uint64_t cnt = 0;
     NQB_TRY(generate_pool_ex(n, depth, nullptr, nullptr, 0, &cnt, nullptr, nullptr));
-    nqb_placement* p = static_cast<nqb_placement*>(std::malloc((cnt ? cnt : 1) * sizeof(nqb_placement)));
+    nqb_placement* p =
+        alloc_fault() ? nullptr : static_cast<nqb_placement*>(std::malloc((cnt ? cnt : 1) * sizeof(nqb_placement)));
     if (!p) return NQB_E_NOMEM;
     uint64_t got = 0;
     const int s = generate_pool_ex(n, depth, nullptr, p, cnt, &got, nullptr, nullptr);
@@ -94,7 +97,7 @@ int nqb_generate_pool_placements(unsigned n, unsigned depth, nqb_placement** pla
     *placements = p;
     *count = got;
     return NQB_OK;
-}
+} NQB_ABI_CATCH
 
 int nqb_states_from_placements(const nqb_placement* placements, uint64_t count, int mirror_weight, nqb_state* out) {
     if (count && (!placements || !out)) return NQB_E_INVALID;
@@ -121,7 +124,7 @@ int nqb_states_from_placements(const nqb_placement* placements, uint64_t count, 
 }
 
 int nqb_write_state_file(const char* path, const nqb_placement* placements, uint64_t count, unsigned n,
-                         unsigned locked_row, int header) {
+                         unsigned locked_row, int header) try {
     if (!path || !placements || count == 0 || n < NQB_MIN_N || n > NQB_MAX_N || locked_row > 255)
         return NQB_E_INVALID;
     uint64_t per_row[kMaxRow + 1] = {};
@@ -129,9 +132,10 @@ int nqb_write_state_file(const char* path, const nqb_placement* placements, uint
         if (placements[i].n != n || !placement_ok(placements[i])) return NQB_E_INVALID;
         per_row[placements[i].row]++;
     }
+    Out o(nullptr);
     FILE* f = std::fopen(path, "wb");
     if (!f) return NQB_E_IO;
-    Out o(f);
+    o.f = f;
     if (header) {
         o.put<uint32_t>(NQB_STATE_FILE_VERSION);
         o.put<uint64_t>(NQB_STATE_FILE_FLAGS);
@@ -150,13 +154,16 @@ int nqb_write_state_file(const char* path, const nqb_placement* placements, uint
     const bool bad = o.bad || std::ferror(f);
     if (std::fclose(f) != 0 || bad) return NQB_E_IO;
     return NQB_OK;
-}
+} NQB_ABI_CATCH
 
 int nqb_read_state_file(const char* path, int header, unsigned expect_n, nqb_state_file* info,
-                        nqb_placement** placements) {
+                        nqb_placement** placements) try {
     if (!path || !info || !placements) return NQB_E_INVALID;
     std::memset(info, 0, sizeof(*info));
     *placements = nullptr;
+    const uint64_t chunk = 1u << 16;  // boards per read
+    std::vector<uint8_t> cols;
+    cols.reserve(chunk * kMaxRow);  // before the file is open: nothing below throws
     FILE* f = std::fopen(path, "rb");
     if (!f) return NQB_E_IO;
     std::fseek(f, 0, SEEK_END);
@@ -181,7 +188,6 @@ int nqb_read_state_file(const char* path, int header, unsigned expect_n, nqb_sta
     if (n8 < NQB_MIN_N || n8 > NQB_MAX_N) return fail(NQB_E_FORMAT);
     if (expect_n && n8 != expect_n) return fail(NQB_E_INVALID);
     uint64_t filled = 0, cap = 0;
-    std::vector<uint8_t> cols;
     for (;;) {
         uint8_t r = 0;
         if (std::fread(&r, 1, 1, f) != 1) break;  // end of file between segments
@@ -193,13 +199,13 @@ int nqb_read_state_file(const char* path, int header, unsigned expect_n, nqb_sta
         // boards of row 0 carry none, so their count has a fixed bound instead.
         if (r ? cnt > left / r : cnt > kMaxRow0Boards) return fail(NQB_E_FORMAT);
         if (cnt > kMaxPlacements - filled) return fail(NQB_E_FORMAT);
-        const uint64_t chunk = 1u << 16;  // states per read
         for (uint64_t done = 0; done < cnt;) {
             const uint64_t k = cnt - done < chunk ? cnt - done : chunk;
             if (filled + done + k > cap) {  // grow as boards arrive, at most to the segment's end
                 uint64_t want = cap * 2 > filled + cnt ? filled + cnt : cap * 2;
                 if (want < filled + done + k) want = filled + done + k;
-                nqb_placement* q = static_cast<nqb_placement*>(std::realloc(p, want * sizeof(nqb_placement)));
+                nqb_placement* q = alloc_fault() ? nullptr
+                                                 : static_cast<nqb_placement*>(std::realloc(p, want * sizeof(nqb_placement)));
                 if (!q) return fail(NQB_E_NOMEM);
                 p = q;
                 cap = want;
@@ -224,13 +230,13 @@ int nqb_read_state_file(const char* path, int header, unsigned expect_n, nqb_sta
     if (std::ferror(f)) return fail(NQB_E_IO);
     if (filled != total) return fail(NQB_E_FORMAT);
     std::fclose(f);
-    if (!p) p = static_cast<nqb_placement*>(std::malloc(sizeof(nqb_placement)));
+    if (!p && !alloc_fault()) p = static_cast<nqb_placement*>(std::malloc(sizeof(nqb_placement)));
     if (!p) return NQB_E_NOMEM;
     *placements = p;
     return NQB_OK;
-}
+} NQB_ABI_CATCH
 
-int nqb_pool_for_target(unsigned n, uint64_t how_many, nqb_target* t) {
+int nqb_pool_for_target(unsigned n, uint64_t how_many, nqb_target* t) try {
     if (!t || n < NQB_MIN_N || n > NQB_MAX_N || how_many == 0) return NQB_E_INVALID;
     std::memset(t, 0, sizeof(*t));
     // the reference's arithmetic, in double as it does it (n_queens.cu:135-139)
@@ -269,6 +275,6 @@ int nqb_pool_for_target(unsigned n, uint64_t how_many, nqb_target* t) {
     t->pool_depth = a_lock == 1 ? 2 : a_lock;
     t->count = a_total;
     return NQB_OK;
-}
+} NQB_ABI_CATCH
 
 }  // extern "C"

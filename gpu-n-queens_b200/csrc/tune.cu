@@ -72,7 +72,7 @@ int time_candidate(const nqb_state* d_sample, uint32_t count, unsigned depth, co
 using namespace nqb;
 
 extern "C" int nqb_tune_count(unsigned n, const unsigned* depths, unsigned n_depths, const nqb_opts* opts,
-                              unsigned sample_div, nqb_tune_result* out) {
+                              unsigned sample_div, nqb_tune_result* out) try {
     if (!out || !depths || n_depths == 0 || sample_div == 0) return NQB_E_INVALID;
     std::memset(out, 0, sizeof(*out));
     nqb_opts base;
@@ -80,15 +80,6 @@ extern "C" int nqb_tune_count(unsigned n, const unsigned* depths, unsigned n_dep
     if (opts) base = *opts;
     for (unsigned k = 0; k < n_depths; ++k)
         if (n < NQB_MIN_N || n > NQB_MAX_N || depths[k] < 1 || depths[k] >= n) return NQB_E_INVALID;
-    NQB_TRY(nqb_device_check(base.device));
-    int prev = 0;
-    cudaGetDevice(&prev);
-    int st = cuda_status(cudaSetDevice(base.device));
-    cudaStream_t s = nullptr;
-    if (!st) st = cuda_status(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-    unsigned long long* d_out = nullptr;
-    if (!st) st = dev_alloc(&d_out, 8 * sizeof(unsigned long long) + kBatchedScratchBytes, s);  // results, scratch
-
     std::vector<Candidate> cands;
     for (int form : {NQB_FORM_PLAIN, NQB_FORM_BATCHED})
         for (int block : {64, 128, 256}) {
@@ -98,6 +89,27 @@ extern "C" int nqb_tune_count(unsigned n, const unsigned* depths, unsigned n_dep
                 cands.push_back({form, block, 0});
             }
         }
+    NQB_TRY(nqb_device_check(base.device));
+    struct Held {  // released on every way out, an exception included
+        int prev = 0;
+        cudaStream_t s = nullptr;
+        unsigned long long* d_out = nullptr;
+        ~Held() {
+            if (d_out) dev_free(d_out, s);
+            if (s) {
+                cudaStreamSynchronize(s);
+                cudaStreamDestroy(s);
+            }
+            cudaSetDevice(prev);
+        }
+    } held;
+    cudaGetDevice(&held.prev);
+    int st = cuda_status(cudaSetDevice(base.device));
+    if (!st) st = cuda_status(cudaStreamCreateWithFlags(&held.s, cudaStreamNonBlocking));
+    const cudaStream_t s = held.s;
+    if (!st) st = dev_alloc(&held.d_out, 8 * sizeof(unsigned long long) + kBatchedScratchBytes, s);  // results, scratch
+    unsigned long long* const d_out = held.d_out;
+
     out->sample_div = sample_div;
     out->best_ms = -1.0;
     for (unsigned k = 0; k < n_depths && !st; ++k) {
@@ -144,11 +156,5 @@ extern "C" int nqb_tune_count(unsigned n, const unsigned* depths, unsigned n_dep
         }
         if (d_sample) dev_free(d_sample, s);
     }
-    if (d_out) dev_free(d_out, s);
-    if (s) {
-        cudaStreamSynchronize(s);
-        cudaStreamDestroy(s);
-    }
-    cudaSetDevice(prev);
     return st;
-}
+} NQB_ABI_CATCH

@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define NQB_VERSION 10100 /* 1.1.0 */
+#define NQB_VERSION 10200 /* 1.2.0 */
 
 /* Board sizes.  The reference accepts 7 < N < 32 (deffinitions.cuh:116-118);
  * this library accepts 4..31.  Counts are exact in uint64 up to N = 28. */
@@ -140,6 +140,17 @@ int nqb_device_check(int device);
  * own stream-ordered memory pool on that device and stay cached for the next call instead
  * of being unmapped; this returns the cached memory of `device` to the driver. */
 int nqb_trim_device_memory(int device);
+
+/* Test hook for the error paths: makes one allocation of the library fail as if memory had
+ * run out.  after >= 0: the library's next `after` allocations succeed and the one after
+ * them fails (once; the hook is then off); after < 0 turns the hook off.  Counted are the
+ * library's own device buffers, pinned host buffers and host arrays (pools, state-file
+ * placements), from every thread; allocations inside the C++ standard library are not.
+ * Returns the countdown it replaces: -1 when the hook was off or has fired, else the number
+ * of allocations that were still to succeed.  A call whose allocation fails returns
+ * NQB_E_NOMEM, releases what it had allocated and leaves the library usable; no entry point
+ * lets a C++ exception escape (one from the standard library is NQB_E_NOMEM too). */
+long long nqb_debug_fail_allocation(long long after);
 
 /* Measures the integer lane-ops per second `device` sustains (the search kernels'
  * roofline denominator): every SM at full occupancy running independent chains of one

@@ -19,7 +19,7 @@ def test_library_loads_and_exports_header(nqb):
 
 
 def test_version_and_strerror(nqb):
-    assert nqb.lib().nqb_version() == 10100
+    assert nqb.lib().nqb_version() == 10200
     for s in range(9):
         assert nqb.strerror(s) not in ("", "unknown status")
     assert nqb.strerror(99) == "unknown status"
