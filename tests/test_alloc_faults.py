@@ -103,3 +103,89 @@ def test_state_file_reader_frees_on_failure(nqb, tmp_path):
     finally:
         nqb.debug_fail_allocation(-1)
     assert st == nqb.E_NOMEM and not p.value
+
+
+# ---- device paths: pools, launches, schedules, plans, the tuner and the cost model ----
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("form,host_pool", [(0, False), (1, False), (0, True), (1, True)])
+def test_count_allocation_failure(nqb, form, host_pool):
+    c0, st0 = nqb.count_ex(14, 4, form=form, host_pool=host_pool)
+    hit, last = _sweep(nqb, lambda: _status(lambda: nqb.count_ex(14, 4, form=form, host_pool=host_pool)))
+    assert hit and set(hit) == {nqb.E_NOMEM} and last == nqb.OK
+    c, st = nqb.count_ex(14, 4, form=form, host_pool=host_pool)
+    assert c == c0 == KAT[14] and st["nodes"] == st0["nodes"]
+
+
+@pytest.mark.gpu
+def test_autotuned_count_allocation_failure(nqb):
+    hit, last = _sweep(nqb, lambda: _status(lambda: nqb.count_ex(14, 4, autotune=True)))
+    assert len(hit) >= 3 and set(hit) == {nqb.E_NOMEM} and last == nqb.OK
+    assert nqb.count_ex(14, 4, autotune=True)[0] == KAT[14]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("sched_cost", [0, 2])
+def test_batch_allocation_failure(nqb, sched_cost):
+    boards = nqb.sample_boards(77, 2000, 10, 14, 2, 5)
+    want, _ = nqb.solve_batch(boards, form=nqb.FORM_BATCHED, sched_cost=sched_cost)
+    hit, last = _sweep(nqb, lambda: _status(
+        lambda: nqb.solve_batch(boards, form=nqb.FORM_BATCHED, sched_cost=sched_cost)))
+    assert hit and set(hit) == {nqb.E_NOMEM} and last == nqb.OK
+    got, _ = nqb.solve_batch(boards, form=nqb.FORM_BATCHED, sched_cost=sched_cost)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.gpu
+def test_plan_allocation_failure(nqb):
+    boards = nqb.sample_boards(78, 3000, 10, 14, 2, 5)
+    want, _ = nqb.solve_batch(boards, form=nqb.FORM_BATCHED)
+
+    def create_and_run():
+        try:
+            plan = nqb.BatchPlan(boards, autotune=True, sched_cost=2)
+        except nqb.NQBError as e:
+            return e.status
+        try:
+            got, _ = plan.run()
+        finally:
+            plan.close()
+        assert np.array_equal(got, want)
+        return nqb.OK
+
+    hit, last = _sweep(nqb, create_and_run)
+    assert len(hit) >= 6 and set(hit) == {nqb.E_NOMEM} and last == nqb.OK
+    assert create_and_run() == nqb.OK
+
+
+@pytest.mark.gpu
+def test_tuner_allocation_failure(nqb):
+    hit, last = _sweep(nqb, lambda: _status(lambda: nqb.tune_count(14, [3, 4], sample_div=4)))
+    assert len(hit) >= 3 and set(hit) == {nqb.E_NOMEM} and last == nqb.OK
+
+
+@pytest.mark.gpu
+def test_model_allocation_failure(nqb):
+    boards = nqb.sample_boards(79, 512, 10, 13, 2, 5)
+    targets = np.linspace(1.0, 9.0, len(boards)).astype(np.float32)
+
+    def create():
+        try:
+            nqb.Model(device=0, seed=1).close()
+        except nqb.NQBError as e:
+            return e.status
+        return nqb.OK
+
+    hit, last = _sweep(nqb, create)
+    assert len(hit) == 6 and set(hit) == {nqb.E_NOMEM} and last == nqb.OK
+    m = nqb.Model(device=0, seed=1)
+    try:
+        hit, last = _sweep(nqb, lambda: _status(lambda: m.train(boards, targets, epochs=1, batch=256)))
+        assert len(hit) >= 10 and set(hit) == {nqb.E_NOMEM} and last == nqb.OK
+        p0 = m.predict(boards)
+        hit, last = _sweep(nqb, lambda: _status(lambda: m.predict(boards)))
+        assert len(hit) >= 3 and set(hit) == {nqb.E_NOMEM} and last == nqb.OK
+        assert np.array_equal(m.predict(boards), p0)
+    finally:
+        m.close()
