@@ -522,8 +522,8 @@ void nqb_batch_plan_destroy(nqb_batch_plan* plan);
  * nqb_batched_launch_ex (warps share work only inside themselves).
  *
  * - The first call on a device looks the array's device address up
- *   (cudaGetSymbolAddress) with that device current; make that first call before any
- *   stream capture on the device.  The address is kept per device and context: after a
+ *   (cudaGetSymbolAddress) with that device current, which loads the library's module on
+ *   the device if nothing has yet.  The address is kept per device and context: after a
  *   device reset (cudaDeviceReset) the next call looks it up again, so that call is a
  *   first call too.
  * - Each call clears the queue head on `stream` before launching (the array keeps
