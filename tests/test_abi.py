@@ -164,3 +164,27 @@ int main(int argc, char** argv) {
     assert p.returncode == 0 and p.stdout.strip() == "lock 4 states 697", (p.returncode, p.stdout, p.stderr)
     golden = os.path.join(ROOT, "tests", "golden", "nqsf", "g_n10_1334.nqsf")
     assert (tmp_path / "pool.nqsf").read_bytes() == open(golden, "rb").read()  # the reference CLI's -g 1334
+
+
+# Entry points that cannot throw: no standard-library container, `new` or thread on their path
+# (nqb_count only forwards to nqb_count_ex).
+_NO_THROW = {"nqb_version", "nqb_device_count", "nqb_device_check", "nqb_trim_device_memory",
+             "nqb_states_from_ref", "nqb_states_from_placements", "nqb_model_get_params",
+             "nqb_model_set_params", "nqb_batch_plan_run", "nqb_batch_plan_config", "nqb_debug_fail_allocation",
+             "nqb_count"}
+
+
+def test_entry_points_catch_exceptions(nqb):
+    # every entry point returning a status is a function-try-block closed by NQB_ABI_CATCH, so
+    # no C++ exception crosses the C ABI (a source check: the body ends in the handler)
+    import re
+    csrc = os.path.join(os.path.dirname(nqb.__file__), "csrc")
+    src = "".join(open(os.path.join(csrc, f)).read() for f in sorted(os.listdir(csrc))
+                  if f.endswith((".cu", ".cpp")))
+    header = open(os.path.join(os.path.dirname(os.path.dirname(nqb.__file__)), "include", "nqb.h")).read()
+    status_fns = set(re.findall(r"^(?:int|long long) (nqb_\w+)\(", header, re.M))
+    assert len(status_fns) > 40
+    missing = [name for name in sorted(status_fns - _NO_THROW)
+               if not re.search(r"^(?:extern \"C\" )?(?:int|long long) " + name +
+                                r"\([^{;]*\) try \{\n(?:(?!^\}).*\n)*?\} NQB_ABI_CATCH$", src, re.M)]
+    assert not missing, f"not function-try-blocks closed by NQB_ABI_CATCH: {missing}"
