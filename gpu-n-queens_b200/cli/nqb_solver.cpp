@@ -21,6 +21,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <exception>
 #include <string>
 #include <utility>
 #include <vector>
@@ -306,9 +307,7 @@ std::vector<nqb_state> to_states(const LibArray<nqb_placement>& pl, int* status)
     return st;
 }
 
-}  // namespace
-
-int main(int argc, char** argv) {
+int run(int argc, char** argv) {
     Args a;
     const int pr = parse(argc, argv, &a);
     if (pr >= 0) return pr;
@@ -377,4 +376,15 @@ int main(int argc, char** argv) {
     if (s) return nqb_fail("Failed to generate states", s);
     std::printf("%" PRIu64 " states generated.\n", st.size());
     return solve_and_print(st.data(), st.size(), a.n, a);
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    try {
+        return run(argc, argv);
+    } catch (const std::exception& e) {  // the standard library ran out of host memory or threads
+        std::fprintf(stderr, "nqb_solver: %s\n", e.what());
+        return EXIT_FAILURE;
+    }
 }
