@@ -24,8 +24,9 @@ import pytest
 
 
 class Model:
-    def __init__(self, seed, warps, cap, items, donate_every=3):
+    def __init__(self, seed, warps, cap, items, donate_every=3, early_unregister=False):
         self.rng = random.Random(seed)
+        self.early_unregister = early_unregister  # the variant that leaves the hungry count first
         self.cap = cap
         self.head = self.tail = 0
         self.turn = [0] * cap
@@ -95,11 +96,16 @@ class Model:
                 yield
                 if t != h:
                     want = min(t - h, 32)
+                    if self.early_unregister:  # leave the hungry count before the take
+                        self.hungry -= 1
+                        yield
                     if self.head != h:  # another warp took rows first
+                        if self.early_unregister:
+                            self.hungry += 1
                         yield
                         continue
                     self.head = h + want
-                    self.holding[w] = True
+                    self.holding[w] = True  # rows taken, not yet being searched
                     yield
                     for j in range(want):
                         idx = h + j
@@ -110,7 +116,8 @@ class Model:
                         self.slot[idx % self.cap] = None
                         self.turn[idx % self.cap] = 2 * lap + 2
                         yield
-                    self.hungry -= 1
+                    if not self.early_unregister:
+                        self.hungry -= 1
                     self.holding[w] = False
                     yield
                     break
@@ -135,14 +142,15 @@ class Model:
         raise AssertionError("the model did not terminate")
 
 
+@pytest.mark.parametrize("early_unregister", [False, True])
 @pytest.mark.parametrize("seed", range(60))
-def test_steal_protocol_is_exact_under_any_interleaving(seed):
+def test_steal_protocol_is_exact_under_any_interleaving(seed, early_unregister):
     rng = random.Random(1000 + seed)
     warps = rng.choice([2, 3, 4, 6, 8])
     cap = rng.choice([2, 4, 8, 64])
     # uneven items: most warps get little, a few get long subtrees
     items = [rng.choice([0, 1, 3, 10, 200, 1500]) for _ in range(warps * rng.choice([1, 2, 3]))]
-    m = Model(seed, warps, cap, items, donate_every=rng.choice([1, 3, 16]))
+    m = Model(seed, warps, cap, items, donate_every=rng.choice([1, 3, 16]), early_unregister=early_unregister)
     m.run()
     assert m.done_units == sum(items)       # every unit once: no row lost or duplicated
     assert m.head == m.tail                 # the ring is empty at the end
@@ -170,3 +178,14 @@ def test_termination_window_keeps_the_count():
         assert m.done_units == 1360 and m.head == m.tail
         windows += m.window_exits
     assert windows > 0
+
+
+def test_leaving_the_hungry_count_before_the_take_closes_the_window():
+    # the variant (not built in the kernel): a poller leaves the hungry count before its
+    # compare-and-swap on the head and joins it again if that fails; no warp then leaves while
+    # another holds taken rows, and the count stays exact
+    for seed in range(40):
+        m = Model(seed, 6, 8, [400, 5, 5, 900, 0, 50], donate_every=1, early_unregister=True)
+        m.run()
+        assert m.done_units == 1360 and m.head == m.tail and m.hungry == m.started
+        assert m.window_exits == 0
